@@ -1,0 +1,241 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes front end of the oracle (oracle.cpp).
+
+The oracle is a CPU restatement of tenrso's CP-ALS hot path. Only tests/,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this
+module, always as the checker or as the timed CPU baseline, never as the
+product. Citations (paths inside the tenrso repository) are in oracle.cpp.
+
+Parity anchors: the golden vectors in tenrso's own unit tests (Khatri-Rao
+``khatri_rao.rs:41-55,479-554``; MTTKRP definition ``mttkrp.rs:1000-1043``;
+Gram ``cp/tests.rs:26-35``; COO ``coo.rs:420-452``; CSF ``csf.rs:501-682``)
+are replayed against this oracle in tests/test_oracle.py. The least-squares
+solve (``scirs2_linalg::lstsq`` 0.3.0, a crates.io dependency that is not
+vendored) is restated as a Cholesky solve; no reference test pins a solve
+value, so that step is "parity unpinned".
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile."""
+    if force or not os.path.exists(_LIB) or (
+        os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "oracle.cpp"))
+    ):
+        subprocess.run(["make", "-B", "-C", _HERE, "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(_LIB)
+        P = C.c_void_p
+        I64 = C.c_int64
+        L.orc_mttkrp_f32.argtypes = [P, C.c_int, P, P, I64, C.c_int, P, C.c_int]
+        L.orc_mttkrp_f64.argtypes = [P, C.c_int, P, P, I64, C.c_int, P, C.c_int]
+        L.orc_khatri_rao_f64.argtypes = [P, I64, P, I64, I64, P]
+        L.orc_gram_f64.argtypes = [P, I64, I64, P]
+        L.orc_cp_als_f32.argtypes = [P, C.c_int, P, I64, C.c_int, C.c_double, P, P, P, P, P, P, P,
+                                     C.c_int]
+        L.orc_cp_als_f64.argtypes = L.orc_cp_als_f32.argtypes
+        L.orc_solve_f64.argtypes = [P, I64, P, I64, P]
+        L.orc_coo_dedup_f32.argtypes = [P, P, I64, C.c_int]
+        L.orc_coo_dedup_f32.restype = I64
+        L.orc_csf_from_coo_f32.argtypes = [P, P, I64, C.c_int, P, P, P, P, P]
+        L.orc_coo_mttkrp_f64.argtypes = [P, P, I64, C.c_int, P, P, I64, C.c_int, P]
+        L.orc_cp_reconstruct_f64.argtypes = [P, C.c_int, P, I64, P, P]
+        L.orc_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ptr_array(arrs):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def mttkrp(X: np.ndarray, factors, mode: int, faithful: bool = False) -> np.ndarray:
+    """Restated ``tenrso_kernels::mttkrp`` (mttkrp.rs:74-146) in X's dtype."""
+    dt = X.dtype
+    assert dt in (np.float32, np.float64)
+    X = np.ascontiguousarray(X)
+    fs = [np.ascontiguousarray(f, dtype=dt) for f in factors]
+    shape = np.asarray(X.shape, dtype=np.int64)
+    R = fs[0].shape[1]
+    out = np.zeros((X.shape[mode], R), dtype=dt)
+    fn = lib().orc_mttkrp_f32 if dt == np.float32 else lib().orc_mttkrp_f64
+    rc = fn(_ptr(X), X.ndim, _ptr(shape), _ptr_array(fs), R, mode, _ptr(out), int(faithful))
+    if rc:
+        raise ValueError(f"oracle mttkrp failed: {rc}")
+    return out
+
+
+def khatri_rao(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """Restated ``tenrso_kernels::khatri_rao`` (khatri_rao.rs:56-89)."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    assert A.shape[1] == B.shape[1]
+    out = np.zeros((A.shape[0] * B.shape[0], A.shape[1]))
+    lib().orc_khatri_rao_f64(_ptr(A), A.shape[0], _ptr(B), B.shape[0], A.shape[1], _ptr(out))
+    return out
+
+
+def gram(F: np.ndarray) -> np.ndarray:
+    """Restated ``compute_gram_matrix`` (cp/helpers.rs:434-452)."""
+    F = np.ascontiguousarray(F, dtype=np.float64)
+    G = np.zeros((F.shape[1], F.shape[1]))
+    lib().orc_gram_f64(_ptr(F), F.shape[0], F.shape[1], _ptr(G))
+    return G
+
+
+def solve(M: np.ndarray, G: np.ndarray) -> np.ndarray:
+    """Restated ``solve_least_squares`` (cp/helpers.rs:455-495), FP64."""
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    out = np.zeros_like(M)
+    rc = lib().orc_solve_f64(_ptr(M), M.shape[0], _ptr(G), G.shape[0], _ptr(out))
+    if rc:
+        raise np.linalg.LinAlgError("oracle solve: Gram not positive definite")
+    return out
+
+
+REASONS = ("MaxIterations", "FitTolerance", "Oscillation", "TimeLimit")
+
+
+def cp_als(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
+           faithful: bool = False):
+    """Restated ``tenrso_decomp::cp_als`` (cp/core.rs:91-214) from injected
+    factors. Returns (factors, info dict)."""
+    dt = X.dtype
+    X = np.ascontiguousarray(X)
+    shape = np.asarray(X.shape, dtype=np.int64)
+    flat = np.concatenate([np.ascontiguousarray(f, dtype=dt).ravel() for f in init_factors])
+    hist = np.zeros(max(max_iters, 1), dtype=dt)
+    iters = C.c_int(0)
+    reason = C.c_int(0)
+    osc = C.c_int(0)
+    ctype = C.c_float if dt == np.float32 else C.c_double
+    change = ctype(0)
+    fit = ctype(0)
+    fn = lib().orc_cp_als_f32 if dt == np.float32 else lib().orc_cp_als_f64
+    rc = fn(_ptr(X), X.ndim, _ptr(shape), rank, max_iters, float(tol), _ptr(flat), _ptr(hist),
+            C.byref(iters), C.byref(reason), C.byref(osc), C.byref(change), C.byref(fit),
+            int(faithful))
+    if rc == -10:
+        raise ValueError(f"Invalid rank: {rank}")
+    if rc == -11:
+        raise ValueError(f"Invalid tolerance: {tol}")
+    if rc:
+        raise np.linalg.LinAlgError(f"oracle cp_als failed: {rc}")
+    out, off = [], 0
+    for n in X.shape:
+        out.append(flat[off:off + n * rank].reshape(n, rank).copy())
+        off += n * rank
+    info = dict(fit=float(fit.value), iters=iters.value, reason=REASONS[reason.value],
+                oscillation_count=osc.value, oscillated=osc.value > 0,
+                final_fit_change=float(change.value), fit_history=hist[:iters.value].copy())
+    return out, info
+
+
+def coo_deduplicate(idx: np.ndarray, vals: np.ndarray):
+    """Restated ``CooTensor::deduplicate`` (coo.rs:320-347)."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64).copy()
+    vals = np.ascontiguousarray(vals, dtype=np.float32).copy()
+    n = lib().orc_coo_dedup_f32(_ptr(idx), _ptr(vals), idx.shape[0], idx.shape[1])
+    return idx[:n].copy(), vals[:n].copy()
+
+
+def csf_from_coo(idx: np.ndarray, vals: np.ndarray, mode_order):
+    """Restated ``CsfTensor::from_coo`` (csf.rs:137-264). Returns
+    (fptr list, fids list, vals) with the reference's nnz-offset fptr."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    vals = np.ascontiguousarray(vals, dtype=np.float32)
+    nnz, ndim = idx.shape
+    mo = np.asarray(mode_order, dtype=np.int64)
+    if mo.shape[0] != ndim:
+        raise ValueError("Invalid mode order: length mismatch")
+    fptr = np.zeros((ndim, nnz + 1), dtype=np.int64)
+    fids = np.zeros((ndim, max(nnz, 1)), dtype=np.int64)
+    vout = np.zeros(max(nnz, 1), dtype=np.float32)
+    lens = np.zeros(2 * ndim, dtype=np.int64)
+    rc = lib().orc_csf_from_coo_f32(_ptr(idx), _ptr(vals), nnz, ndim, _ptr(mo), _ptr(fptr),
+                                    _ptr(fids), _ptr(vout), _ptr(lens))
+    if rc:
+        raise ValueError("Invalid mode order: not a permutation")
+    fp = [fptr[l, :lens[2 * l]].copy() for l in range(ndim)]
+    fi = [fids[l, :lens[2 * l + 1]].copy() for l in range(ndim)]
+    nv = len(fi[-1]) if ndim > 1 else 0
+    return fp, fi, vout[:nv].copy()
+
+
+def coo_mttkrp(idx, vals, shape, factors, mode):
+    """Sparse MTTKRP definition (no reference implementation), FP64."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    shp = np.asarray(shape, dtype=np.int64)
+    R = fs[0].shape[1]
+    out = np.zeros((shape[mode], R))
+    lib().orc_coo_mttkrp_f64(_ptr(idx), _ptr(vals), idx.shape[0], idx.shape[1], _ptr(shp),
+                             _ptr_array(fs), R, mode, _ptr(out))
+    return out
+
+
+def cp_reconstruct(factors, weights=None):
+    """Restated ``tenrso_kernels::cp_reconstruct`` (outer.rs:223-274), FP64."""
+    fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    shape = np.asarray([f.shape[0] for f in fs], dtype=np.int64)
+    R = fs[0].shape[1]
+    out = np.zeros(tuple(shape))
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    lib().orc_cp_reconstruct_f64(_ptr_array(fs), len(fs), _ptr(shape), R,
+                                 None if w is None else _ptr(w), _ptr(out))
+    return out
+
+
+def cp_reconstruction_grad(factors, grad_output, weights=None):
+    """Restated ``CpReconstructionGrad::compute_factor_gradients``
+    (tenrso-ad/src/grad.rs:81-120): dL/dU_n = unfold(G, n) . KR_{!=n} . diag(w)."""
+    G = np.ascontiguousarray(grad_output, dtype=np.float64)
+    out = []
+    for n in range(G.ndim):
+        g = mttkrp(G, factors, n)
+        if weights is not None:
+            g = g * np.asarray(weights, dtype=np.float64)[None, :]
+        out.append(g)
+    return out
+
+
+def csf_to_coo(fptr, fids, vals, mode_order):
+    """A correct inverse of the reference CSF layout (every fptr level holds
+    nnz offsets into the sorted entry list). The reference's own CsfIterator
+    (csf.rs:423-495) mis-reconstructs fibers holding more than one nonzero,
+    so it is not used as an oracle."""
+    ndim = len(mode_order)
+    nnz = len(fids[-1])
+    out = np.zeros((nnz, ndim), dtype=np.int64)
+    pos = np.arange(nnz)
+    for level in range(ndim - 1):
+        f = np.searchsorted(np.asarray(fptr[level]), pos, side="right") - 1
+        out[:, mode_order[level]] = np.asarray(fids[level])[f]
+    out[:, mode_order[-1]] = np.asarray(fids[-1])
+    return out, np.asarray(vals)
