@@ -1,0 +1,142 @@
+/*
+ * tenrso_b200 — C ABI of a B200-native (sm_100a) CP-ALS hot path for tenrso.
+ *
+ * Every entry point replaces one tenrso function on the CP-ALS path and is
+ * cited below by its file:line inside the tenrso repository. Plain pointers
+ * and sizes only. Unless a name ends in `_dev`, tensor/factor/output pointers
+ * are HOST memory and the call blocks until the result is on the host, as the
+ * synchronous Rust functions do; `_dev` variants take device pointers and are
+ * stream-ordered on the context's stream.
+ *
+ * Layouts: dense tensors are row-major (C order) unless a strides array is
+ * given; factor matrices are row-major I_m x R; outputs are row-major.
+ *
+ * Errors: every function returns a tsr_status. tsr_last_error() returns the
+ * message of the calling thread's last failure, worded as tenrso words it
+ * (e.g. "Mode 5 out of bounds for tensor with rank 2"), so a Rust shim can
+ * re-raise it through anyhow::bail! unchanged.
+ */
+#ifndef TENRSO_B200_H
+#define TENRSO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tsr_status {
+  TSR_OK = 0,
+  TSR_E_MODE_OOB = 1,        /* mttkrp.rs:87-93 "Mode {} out of bounds ..." */
+  TSR_E_NFACTORS = 2,        /* mttkrp.rs:95-101 "Number of factor matrices ..." */
+  TSR_E_RANK_MISMATCH = 3,   /* mttkrp.rs:106-112 "Factor matrix {} has {} columns ..." */
+  TSR_E_ROWS_MISMATCH = 4,   /* mttkrp.rs:113-121 "Factor matrix {} has {} rows ..." */
+  TSR_E_INVALID_RANK = 5,    /* cp/types.rs:15 CpError::InvalidRank */
+  TSR_E_INVALID_TOL = 6,     /* cp/types.rs:18 CpError::InvalidTolerance */
+  TSR_E_NOT_SPD = 7,         /* cp/types.rs:21 CpError::LinalgError */
+  TSR_E_TIMEOUT = 8,         /* a bounded device-side wait gave up */
+  TSR_E_CUDA = 9,            /* CUDA runtime/driver failure */
+  TSR_E_INVALID_ARG = 10,    /* null pointer, bad size, unsupported layout */
+  TSR_E_NEED_2_FACTORS = 11, /* mttkrp.rs:196-198 "Need at least 2 factor matrices for MTTKRP" */
+  TSR_E_TILE_SIZE = 12,      /* mttkrp.rs:402-404 "Tile size must be greater than 0" */
+  TSR_E_MODE_ORDER = 13,     /* csf.rs:143-156 CsfError::InvalidModeOrder */
+  TSR_E_UNSUPPORTED = 14,    /* shape/rank outside what the kernels implement */
+  TSR_E_COLS_MISMATCH = 15,  /* khatri_rao.rs:63-67 "Number of columns must match" */
+  TSR_E_SHAPE = 16,          /* cp/types.rs:24 CpError::ShapeMismatch / coo.rs errors */
+  TSR_E_INDEX_OOB = 17       /* coo.rs:130-137 CooError::IndexOutOfBounds */
+} tsr_status;
+
+/* Arithmetic of the dense MTTKRP. FP32: IEEE fp32 FMA on the SIMT pipes.
+ * BF16X3: operands split as x = hi + lo (both bf16), three tcgen05 bf16 MMAs
+ * (hi*hi + hi*lo + lo*hi) with fp32 accumulation in tensor memory. */
+typedef enum tsr_precision { TSR_PREC_FP32 = 0, TSR_PREC_BF16X3 = 1 } tsr_precision;
+
+/* cp/types.rs:319-328 ConvergenceReason */
+typedef enum tsr_reason {
+  TSR_REASON_MAX_ITERATIONS = 0,
+  TSR_REASON_FIT_TOLERANCE = 1,
+  TSR_REASON_OSCILLATION = 2,
+  TSR_REASON_TIME_LIMIT = 3
+} tsr_reason;
+
+/* cp/types.rs:329-344 ConvergenceInfo + CpDecomp::{fit, iters} (types.rs:350-368).
+ * fit_history is caller-owned with room for max_iters values (may be NULL). */
+typedef struct tsr_cp_info {
+  double fit;
+  int32_t iters;
+  int32_t reason; /* tsr_reason */
+  int32_t oscillated;
+  int32_t oscillation_count;
+  double final_fit_change;
+  double* fit_history;
+  int32_t ridge_used; /* the eps*rank*10 ridge of cp/helpers.rs:477-490 engaged */
+  int32_t reserved;
+} tsr_cp_info;
+
+typedef struct tsr_ctx tsr_ctx;
+
+/* ---- context ----------------------------------------------------------- */
+const char* tsr_last_error(void);
+const char* tsr_status_string(int status);
+const char* tsr_version(void);
+/* stream may be NULL (the context creates its own) or a cudaStream_t. */
+int tsr_ctx_create(int device, void* stream, tsr_ctx** out);
+int tsr_ctx_destroy(tsr_ctx* ctx);
+int tsr_ctx_synchronize(tsr_ctx* ctx);
+/* Kernels launched through this context since creation (a counter). */
+int64_t tsr_ctx_launch_count(const tsr_ctx* ctx);
+
+/* ---- Khatri-Rao: crates/tenrso-kernels/src/khatri_rao.rs:56-89 ----------
+ * out (I*J x K) with row a*J + b = A[a,:] * B[b,:]. Host pointers. */
+int tsr_khatri_rao_f32(tsr_ctx* ctx, const float* a, int64_t a_rows, int64_t a_cols,
+                       const float* b, int64_t b_rows, int64_t b_cols, float* out);
+
+/* ---- dense MTTKRP: crates/tenrso-kernels/src/mttkrp.rs:74-146 -----------
+ * tensor: ndim dims, shape[ndim]; strides[ndim] in elements (NULL = row-major).
+ * factors[m]: factor_rows[m] x factor_cols[m] row-major (ndim_factors of them).
+ * out: shape[mode] x R row-major. Validation order and messages follow
+ * mttkrp.rs:86-122. */
+int tsr_mttkrp_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                   const int64_t* strides, const float* const* factors, int n_factors,
+                   const int64_t* factor_rows, const int64_t* factor_cols, int mode,
+                   int precision, float* out);
+/* mttkrp_blocked / mttkrp_blocked_parallel (mttkrp.rs:395-498, 529-609): the
+ * tile size only regroups the sum; validated (> 0) then the same kernel runs. */
+int tsr_mttkrp_blocked_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                           const int64_t* strides, const float* const* factors, int n_factors,
+                           const int64_t* factor_rows, const int64_t* factor_cols, int mode,
+                           int64_t tile_size, int precision, float* out);
+/* mttkrp_all_modes (crates/tenrso-kernels/src/utils.rs:282-307): out[m] gets
+ * shape[m] x R for every mode m, the tensor is uploaded once. */
+int tsr_mttkrp_all_modes_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                             const float* const* factors, int64_t rank, int precision,
+                             float* const* out);
+/* Device-resident MTTKRP: d_tensor row-major contiguous on the device,
+ * d_factors[m] device pointers (row-major shape[m] x rank), d_out device. */
+int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                       const float* const* d_factors, int64_t rank, int mode, int precision,
+                       float* d_out);
+
+/* ---- CP-ALS: crates/tenrso-decomp/src/cp/core.rs:91-214 -----------------
+ * Same loop, validation (rank in [1, min I_n], tol in [0,1)), fit, oscillation
+ * and convergence rules. init_factors: concatenated row-major I_0xR, I_1xR, ...
+ * (the injected initialisation tenrso cannot seed); NULL = U(0,1) from the
+ * library's SplitMix64 stream `seed` (InitStrategy::Random, helpers.rs:215-222).
+ * time_limit_s < 0 means None. out_factors: concatenated like init_factors. */
+int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                   int64_t rank, int max_iters, double tol, const float* init_factors,
+                   uint64_t seed, int precision, double time_limit_s, float* out_factors,
+                   tsr_cp_info* info);
+/* Device-resident CP-ALS: d_tensor (row-major), d_init and d_out_factors are
+ * device pointers (concatenated factors); info stays on the host. */
+int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                       int64_t rank, int max_iters, double tol, const float* d_init,
+                       int precision, double time_limit_s, float* d_out_factors,
+                       tsr_cp_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENRSO_B200_H */

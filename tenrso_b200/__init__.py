@@ -1,0 +1,25 @@
+"""tenrso_b200 — a B200-native (sm_100a) CP-ALS hot path for tenrso.
+
+The product is the CUDA library libtenrso_b200.so behind the C ABI in
+include/tenrso_b200.h. This package is its Python host mirror (the tests and
+bench.py drive the library through it) plus the seeded input generators.
+"""
+from ._lib import TenrsoError, load  # noqa: F401
+from .dense import (  # noqa: F401
+    Context,
+    ConvergenceInfo,
+    CpDecomp,
+    cp_als,
+    cp_als_dev,
+    default_context,
+    khatri_rao,
+    mttkrp,
+    mttkrp_all_modes,
+    mttkrp_blocked,
+    mttkrp_blocked_parallel,
+    mttkrp_dev,
+    mttkrp_fused,
+    mttkrp_fused_parallel,
+)
+
+__version__ = "0.1.0"

@@ -1,0 +1,97 @@
+"""ctypes binding of libtenrso_b200.so (the C ABI in include/tenrso_b200.h).
+
+The library is the product: there is no CPU fallback. Loading fails loudly
+when the shared object is missing, and every call that reaches a kernel needs
+a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtenrso_b200.so")
+
+P = C.c_void_p
+I64 = C.c_int64
+PI64 = C.POINTER(C.c_int64)
+
+
+class CpInfo(C.Structure):
+    _fields_ = [
+        ("fit", C.c_double),
+        ("iters", C.c_int32),
+        ("reason", C.c_int32),
+        ("oscillated", C.c_int32),
+        ("oscillation_count", C.c_int32),
+        ("final_fit_change", C.c_double),
+        ("fit_history", C.POINTER(C.c_double)),
+        ("ridge_used", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "tsr_last_error": (C.c_char_p, []),
+    "tsr_status_string": (C.c_char_p, [C.c_int]),
+    "tsr_version": (C.c_char_p, []),
+    "tsr_ctx_create": (C.c_int, [C.c_int, P, C.POINTER(P)]),
+    "tsr_ctx_destroy": (C.c_int, [P]),
+    "tsr_ctx_synchronize": (C.c_int, [P]),
+    "tsr_ctx_launch_count": (I64, [P]),
+    "tsr_khatri_rao_f32": (C.c_int, [P, P, I64, I64, P, I64, I64, P]),
+    "tsr_mttkrp_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, P]),
+    "tsr_mttkrp_blocked_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, I64,
+                                         C.c_int, P]),
+    "tsr_mttkrp_all_modes_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, P]),
+    "tsr_mttkrp_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, C.c_int, P]),
+    "tsr_cp_als_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_uint64,
+                                 C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
+    "tsr_cp_als_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_int,
+                                     C.c_double, P, C.POINTER(CpInfo)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the in-tree shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m tenrso_b200.build` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+STATUS = {
+    0: "TSR_OK", 1: "TSR_E_MODE_OOB", 2: "TSR_E_NFACTORS", 3: "TSR_E_RANK_MISMATCH",
+    4: "TSR_E_ROWS_MISMATCH", 5: "TSR_E_INVALID_RANK", 6: "TSR_E_INVALID_TOL",
+    7: "TSR_E_NOT_SPD", 8: "TSR_E_TIMEOUT", 9: "TSR_E_CUDA", 10: "TSR_E_INVALID_ARG",
+    11: "TSR_E_NEED_2_FACTORS", 12: "TSR_E_TILE_SIZE", 13: "TSR_E_MODE_ORDER",
+    14: "TSR_E_UNSUPPORTED", 15: "TSR_E_COLS_MISMATCH", 16: "TSR_E_SHAPE",
+    17: "TSR_E_INDEX_OOB",
+}
+
+
+class TenrsoError(RuntimeError):
+    """A non-OK tsr_status; .status is the code, str() is tenrso's message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+        self.code = STATUS.get(status, str(status))
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = load().tsr_last_error().decode()
+        raise TenrsoError(rc, msg)

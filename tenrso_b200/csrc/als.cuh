@@ -1,0 +1,48 @@
+// FP64 Gram / Cholesky / solve / fit kernels of the ALS sweep.
+#pragma once
+#include "common.cuh"
+
+namespace tsr {
+
+constexpr int kMaxRank = 112;  // two R x R FP64 matrices fit in shared memory
+
+// Device-resident ALS bookkeeping mirroring cp/core.rs:104-198.
+struct AlsState {
+  double xnorm_sq;      // ||X||^2 (FP64)
+  double inner;         // <X, Xhat> accumulated by the last mode's solve
+  double prev_fit;
+  double fit;
+  double final_change;
+  int iter;             // iterations completed
+  int osc;              // oscillation_count
+  int reason;           // tsr_reason
+  int done;             // stop flag: converged, oscillation or error
+  unsigned status;      // DevStatus bits
+  int ridge_used;
+  int pad[2];
+};
+
+struct AlsBuffers {
+  double* grams;    // [N][R][R]   U_m^T U_m
+  double* hadam;    // [N][R][R]   Hadamard of the other Grams (G_n)
+  double* ginv;     // [R][R]      G_n^{-1} of the current mode
+  AlsState* state;
+  double* history;  // [max_iters]
+};
+
+// gram[m] = U^T U (FP64), zeroing first. rows x R row-major fp32 input.
+int launch_gram(tsr_ctx* ctx, const float* U, int64_t rows, int R, double* gram);
+// ||X||^2 into state->xnorm_sq (zeroed first).
+int launch_norm_sq(tsr_ctx* ctx, const float* X, int64_t n, AlsState* state);
+// Hadamard of all Grams except `mode`, Cholesky (ridge fallback), inverse.
+// Also zeroes gram[mode] (about to be recomputed) and, when `last`, state->inner.
+int launch_chol(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int mode, int R, float ridge_eps,
+                bool last);
+// U_mode = (sum of split partials) . G^{-1}; accumulates gram[mode] and,
+// when `last`, <M, U> into state->inner.
+int launch_solve(tsr_ctx* ctx, const AlsBuffers& b, const float* partials, int splits,
+                 int64_t rows, int R, float* U, int mode, bool last);
+// fit, fit_history, oscillation and convergence rules of cp/core.rs:173-198.
+int launch_fit(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int R, double tol);
+
+}  // namespace tsr

@@ -1,0 +1,130 @@
+// Shared definitions for the tenrso_b200 CUDA library: the context object,
+// error reporting in tenrso's wording, device workspace slots and small
+// device helpers. All kernels target sm_100a only.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/tenrso_b200.h"
+
+namespace tsr {
+
+// ---------------------------------------------------------------------------
+// error handling
+// ---------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+
+#define TSR_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e__ = (call);                                                            \
+    if (e__ != cudaSuccess)                                                              \
+      return ::tsr::fail(TSR_E_CUDA, "CUDA error %s at %s:%d: %s", cudaGetErrorName(e__), \
+                         __FILE__, __LINE__, cudaGetErrorString(e__));                   \
+  } while (0)
+
+#define TSR_TRY(expr)        \
+  do {                       \
+    int rc__ = (expr);       \
+    if (rc__ != TSR_OK) return rc__; \
+  } while (0)
+
+// Device-side status word bits (written by kernels, read by the host after a
+// synchronize; no kernel raises an error any other way).
+enum DevStatus : unsigned {
+  DS_OK = 0,
+  DS_NOT_SPD = 1u << 0,      // Gram not positive definite even after the ridge
+  DS_RIDGE_USED = 1u << 1,   // ridge fallback engaged (informational)
+  DS_TIMEOUT = 1u << 2,      // a bounded wait gave up
+  DS_BAD_INDEX = 1u << 3,    // an input index was out of range
+};
+
+// ---------------------------------------------------------------------------
+// context and workspace
+// ---------------------------------------------------------------------------
+struct Buffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+enum Slot {
+  SLOT_UNFOLD0 = 0,   // per-mode unfolded copies (fp32 or bf16 hi)
+  SLOT_UNFOLD_LO = 8,  // per-mode bf16 lo copies
+  SLOT_FACTORS = 16,  // factor matrices (fp32)
+  SLOT_PARTIALS,      // split-K partial MTTKRP results
+  SLOT_GRAMS,         // FP64 Grams / Hadamards / inverses
+  SLOT_STATE,         // ALS state (fit history, flags)
+  SLOT_TENSOR,        // staged input tensor
+  SLOT_OUT,           // staged output
+  SLOT_MISC0,
+  SLOT_MISC1,
+  SLOT_MISC2,
+  SLOT_MISC3,
+  SLOT_SPARSE0,
+  SLOT_SPARSE1 = SLOT_SPARSE0 + 16,
+  SLOT_COUNT = SLOT_SPARSE1 + 16
+};
+
+}  // namespace tsr
+
+struct tsr_ctx {
+  int device = 0;
+  int sm_count = 148;
+  size_t l2_bytes = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  tsr::Buffer slots[tsr::SLOT_COUNT];
+  void* pinned = nullptr;  // pinned host staging (grow-only)
+  size_t pinned_bytes = 0;
+  unsigned* d_status = nullptr;  // device status word
+  int launches = 0;              // kernels launched by this context (counter)
+};
+
+namespace tsr {
+
+// Grow-only device buffer for a slot; contents are not preserved on growth.
+int slot_get(tsr_ctx* ctx, int slot, size_t bytes, void** out);
+int pinned_get(tsr_ctx* ctx, size_t bytes, void** out);
+int check_ctx(tsr_ctx* ctx);
+int read_status(tsr_ctx* ctx, unsigned* out);  // synchronizes the stream
+int reset_status(tsr_ctx* ctx);
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+// Shape bookkeeping for a dense N-way tensor and one of its unfoldings.
+constexpr int kMaxModes = 8;
+struct Unfolding {
+  int ndim;
+  int mode;
+  int64_t rows;     // I_mode
+  int64_t cols;     // prod of the other sizes
+  int64_t ld;       // padded row stride (elements), multiple of 8
+  int n_other;      // ndim - 1
+  int64_t other_size[kMaxModes];  // sizes of the other modes, ascending mode order
+  int other_mode[kMaxModes];
+};
+Unfolding make_unfolding(int ndim, const int64_t* shape, int mode);
+
+// Launch the (fp32) unfold of a row-major dense tensor into X_(mode) with row
+// stride u.ld. Pads columns [cols, ld) with zeros.
+int launch_unfold_f32(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
+                      float* out);
+int launch_unfold_bf16x2(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
+                         __nv_bfloat16* hi, __nv_bfloat16* lo);
+
+// Factor pointer table passed by value to kernels.
+struct FactorTable {
+  const float* ptr[kMaxModes];
+  int64_t rows[kMaxModes];
+};
+
+}  // namespace tsr

@@ -1,0 +1,276 @@
+// Context, error reporting, workspace slots, and the layout kernels that
+// build per-mode unfoldings of a dense tensor in HBM.
+#include "common.cuh"
+
+namespace tsr {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int check_ctx(tsr_ctx* ctx) {
+  if (!ctx) return fail(TSR_E_INVALID_ARG, "null context");
+  TSR_CUDA(cudaSetDevice(ctx->device));
+  return TSR_OK;
+}
+
+int slot_get(tsr_ctx* ctx, int slot, size_t bytes, void** out) {
+  Buffer& b = ctx->slots[slot];
+  if (bytes == 0) bytes = 256;
+  if (b.bytes < bytes) {
+    if (b.ptr) {
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      TSR_CUDA(cudaFree(b.ptr));
+      b.ptr = nullptr;
+      b.bytes = 0;
+    }
+    size_t want = (bytes + 4095) & ~size_t(4095);
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+      b.ptr = nullptr;
+      return fail(TSR_E_CUDA, "cudaMalloc of %zu bytes failed: %s", want, cudaGetErrorString(e));
+    }
+    b.bytes = want;
+  }
+  *out = b.ptr;
+  return TSR_OK;
+}
+
+int pinned_get(tsr_ctx* ctx, size_t bytes, void** out) {
+  if (ctx->pinned_bytes < bytes) {
+    if (ctx->pinned) {
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      TSR_CUDA(cudaFreeHost(ctx->pinned));
+      ctx->pinned = nullptr;
+      ctx->pinned_bytes = 0;
+    }
+    size_t want = (bytes + 4095) & ~size_t(4095);
+    TSR_CUDA(cudaMallocHost(&ctx->pinned, want));
+    ctx->pinned_bytes = want;
+  }
+  *out = ctx->pinned;
+  return TSR_OK;
+}
+
+int read_status(tsr_ctx* ctx, unsigned* out) {
+  TSR_CUDA(cudaMemcpyAsync(out, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int reset_status(tsr_ctx* ctx) {
+  TSR_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+  return TSR_OK;
+}
+
+Unfolding make_unfolding(int ndim, const int64_t* shape, int mode) {
+  Unfolding u{};
+  u.ndim = ndim;
+  u.mode = mode;
+  u.rows = shape[mode];
+  u.cols = 1;
+  u.n_other = 0;
+  for (int m = 0; m < ndim; ++m) {
+    if (m == mode) continue;
+    u.other_mode[u.n_other] = m;
+    u.other_size[u.n_other] = shape[m];
+    u.n_other++;
+    u.cols *= shape[m];
+  }
+  u.ld = round_up(u.cols, 8);
+  return u;
+}
+
+// X viewed as [A][I][B] (A = prod of modes before `mode`, B = prod after);
+// X_(mode)[i][a*B + b] = X[a][i][b]. For B >= 32 rows of B elements are
+// contiguous on both sides: plain coalesced copy, one CTA row per (a, i).
+template <class Store>
+__global__ void unfold_copy_kernel(const float* __restrict__ X, int64_t A, int64_t I, int64_t B,
+                                   int64_t ld, Store store) {
+  int64_t row = blockIdx.x;  // (a, i) pair, a-major
+  int64_t a = row / I, i = row % I;
+  const float* src = X + (a * I + i) * B;
+  int64_t dst = i * ld + a * B;
+  for (int64_t b = threadIdx.x; b < B; b += blockDim.x) store(dst + b, __ldg(src + b));
+}
+
+// Small-B case: 32x32 tiles over (a, i) through shared memory so that both the
+// read (i fastest) and the write (a fastest) are coalesced; loops over b.
+template <class Store>
+__global__ void unfold_transpose_kernel(const float* __restrict__ X, int64_t A, int64_t I,
+                                        int64_t B, int64_t ld, Store store) {
+  __shared__ float tile[32][33];
+  int64_t a0 = (int64_t)blockIdx.y * 32, i0 = (int64_t)blockIdx.x * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int64_t b = 0; b < B; ++b) {
+    for (int r = ty; r < 32; r += 8) {
+      int64_t a = a0 + r, i = i0 + tx;
+      tile[r][tx] = (a < A && i < I) ? __ldg(X + (a * I + i) * B + b) : 0.f;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      int64_t i = i0 + r, a = a0 + tx;
+      if (i < I && a < A) store(i * ld + a * B + b, tile[tx][r]);
+    }
+    __syncthreads();
+  }
+}
+
+struct StoreF32 {
+  float* out;
+  __device__ void operator()(int64_t k, float v) const { out[k] = v; }
+};
+struct StoreBF16x2 {
+  __nv_bfloat16* hi;
+  __nv_bfloat16* lo;
+  __device__ void operator()(int64_t k, float v) const {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[k] = h;
+    lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+};
+
+template <class Store>
+static int launch_unfold(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
+                         Store store) {
+  int64_t A = 1, B = 1;
+  for (int m = 0; m < u.mode; ++m) A *= shape[m];
+  for (int m = u.mode + 1; m < u.ndim; ++m) B *= shape[m];
+  const int64_t I = u.rows;
+  if (B >= 32) {
+    if (A * I > INT32_MAX) return fail(TSR_E_UNSUPPORTED, "unfold: too many rows");
+    unfold_copy_kernel<<<(unsigned)(A * I), 256, 0, ctx->stream>>>(X, A, I, B, u.ld, store);
+  } else {
+    dim3 grid((unsigned)ceil_div(I, 32), (unsigned)ceil_div(A, 32));
+    if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "unfold: grid too large");
+    unfold_transpose_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(X, A, I, B, u.ld, store);
+  }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_unfold_f32(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
+                      float* out) {
+  if (u.ld != u.cols)
+    TSR_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * u.rows * u.ld, ctx->stream));
+  return launch_unfold(ctx, X, shape, u, StoreF32{out});
+}
+
+int launch_unfold_bf16x2(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
+                         __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  if (u.ld != u.cols) {
+    TSR_CUDA(cudaMemsetAsync(hi, 0, 2 * u.rows * u.ld, ctx->stream));
+    TSR_CUDA(cudaMemsetAsync(lo, 0, 2 * u.rows * u.ld, ctx->stream));
+  }
+  return launch_unfold(ctx, X, shape, u, StoreBF16x2{hi, lo});
+}
+
+}  // namespace tsr
+
+using namespace tsr;
+
+extern "C" {
+
+const char* tsr_last_error(void) { return g_last_error.c_str(); }
+
+const char* tsr_version(void) { return "tenrso_b200 0.1.0 (sm_100a)"; }
+
+const char* tsr_status_string(int s) {
+  switch (s) {
+    case TSR_OK: return "ok";
+    case TSR_E_MODE_OOB: return "mode out of bounds";
+    case TSR_E_NFACTORS: return "wrong number of factor matrices";
+    case TSR_E_RANK_MISMATCH: return "factor column mismatch";
+    case TSR_E_ROWS_MISMATCH: return "factor row mismatch";
+    case TSR_E_INVALID_RANK: return "invalid rank";
+    case TSR_E_INVALID_TOL: return "invalid tolerance";
+    case TSR_E_NOT_SPD: return "linear algebra error";
+    case TSR_E_TIMEOUT: return "device wait timed out";
+    case TSR_E_CUDA: return "CUDA error";
+    case TSR_E_INVALID_ARG: return "invalid argument";
+    case TSR_E_NEED_2_FACTORS: return "need at least 2 factor matrices";
+    case TSR_E_TILE_SIZE: return "tile size must be greater than 0";
+    case TSR_E_MODE_ORDER: return "invalid mode order";
+    case TSR_E_UNSUPPORTED: return "unsupported shape or rank";
+    case TSR_E_COLS_MISMATCH: return "number of columns must match";
+    case TSR_E_SHAPE: return "shape mismatch";
+    case TSR_E_INDEX_OOB: return "index out of bounds";
+    default: return "unknown status";
+  }
+}
+
+int tsr_ctx_create(int device, void* stream, tsr_ctx** out) {
+  if (!out) return fail(TSR_E_INVALID_ARG, "null output pointer");
+  *out = nullptr;
+  TSR_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  TSR_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(TSR_E_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a",
+                device, prop.major, prop.minor);
+  tsr_ctx* c = new tsr_ctx();
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  c->l2_bytes = prop.l2CacheSize;
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete c;
+      return fail(TSR_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    c->own_stream = true;
+  }
+  cudaError_t e = cudaMalloc(&c->d_status, 256);
+  if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, 256);
+  if (e != cudaSuccess) {
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return fail(TSR_E_CUDA, "status alloc: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return TSR_OK;
+}
+
+int tsr_ctx_destroy(tsr_ctx* ctx) {
+  if (!ctx) return TSR_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->slots)
+    if (b.ptr) cudaFree(b.ptr);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TSR_OK;
+}
+
+int tsr_ctx_synchronize(tsr_ctx* ctx) {
+  TSR_TRY(check_ctx(ctx));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int64_t tsr_ctx_launch_count(const tsr_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,461 @@
+// Host mirror of tenrso's dense CP-ALS entry points over the C ABI:
+//   tenrso_kernels::khatri_rao       khatri_rao.rs:56-89
+//   tenrso_kernels::mttkrp (+blocked, all_modes)  mttkrp.rs:74-146, 395-498; utils.rs:282-307
+//   tenrso_decomp::cp_als            cp/core.rs:91-214
+// Validation order and messages follow the cited lines so that a Rust shim can
+// surface them through anyhow / CpError unchanged.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "als.cuh"
+#include "mttkrp.cuh"
+
+namespace tsr {
+
+namespace {
+
+// mttkrp.rs:86-122 then the KR helper's bail (mttkrp.rs:196-198).
+int validate_mttkrp(int ndim, const int64_t* shape, int n_factors, const int64_t* frows,
+                    const int64_t* fcols, int mode) {
+  if (mode < 0 || mode >= ndim)
+    return fail(TSR_E_MODE_OOB, "Mode %d out of bounds for tensor with rank %d", mode, ndim);
+  if (n_factors != ndim)
+    return fail(TSR_E_NFACTORS, "Number of factor matrices (%d) must match tensor rank (%d)",
+                n_factors, ndim);
+  int64_t R = fcols[0];
+  for (int i = 0; i < ndim; ++i) {
+    if (fcols[i] != R)
+      return fail(TSR_E_RANK_MISMATCH, "Factor matrix %d has %lld columns, expected %lld", i,
+                  (long long)fcols[i], (long long)R);
+    if (frows[i] != shape[i])
+      return fail(TSR_E_ROWS_MISMATCH,
+                  "Factor matrix %d has %lld rows, expected %lld (tensor mode-%d size)", i,
+                  (long long)frows[i], (long long)shape[i], i);
+  }
+  if (ndim < 2) return fail(TSR_E_NEED_2_FACTORS, "Need at least 2 factor matrices for MTTKRP");
+  if (ndim > kMaxModes)
+    return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", ndim, kMaxModes);
+  return TSR_OK;
+}
+
+int64_t numel(int ndim, const int64_t* shape) {
+  int64_t n = 1;
+  for (int d = 0; d < ndim; ++d) n *= shape[d];
+  return n;
+}
+
+bool is_row_major(int ndim, const int64_t* shape, const int64_t* strides) {
+  if (!strides) return true;
+  int64_t s = 1;
+  for (int d = ndim - 1; d >= 0; --d) {
+    if (shape[d] != 1 && strides[d] != s) return false;
+    s *= shape[d];
+  }
+  return true;
+}
+
+// ndarray's as_standard_layout (mttkrp.rs:172-173): pack a strided host view.
+void pack_host(const float* src, int ndim, const int64_t* shape, const int64_t* strides,
+               float* dst) {
+  int64_t n = numel(ndim, shape);
+  std::vector<int64_t> idx(ndim, 0);
+  for (int64_t k = 0; k < n; ++k) {
+    int64_t off = 0;
+    for (int d = 0; d < ndim; ++d) off += idx[d] * strides[d];
+    dst[k] = src[off];
+    for (int d = ndim - 1; d >= 0; --d) {
+      if (++idx[d] < shape[d]) break;
+      idx[d] = 0;
+    }
+  }
+}
+
+// Upload a host tensor (any strides) into a device slot as row-major fp32.
+int upload_tensor(tsr_ctx* ctx, const float* host, int ndim, const int64_t* shape,
+                  const int64_t* strides, float** d_out) {
+  int64_t n = numel(ndim, shape);
+  void* d;
+  TSR_TRY(slot_get(ctx, SLOT_TENSOR, sizeof(float) * n, &d));
+  if (is_row_major(ndim, shape, strides)) {
+    TSR_CUDA(cudaMemcpyAsync(d, host, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    void* stage;
+    TSR_TRY(pinned_get(ctx, sizeof(float) * n, &stage));
+    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+    pack_host(host, ndim, shape, strides, (float*)stage);
+    TSR_CUDA(cudaMemcpyAsync(d, stage, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  *d_out = (float*)d;
+  return TSR_OK;
+}
+
+// Per-mode operand of the MTTKRP: unfolding copies in the precision needed.
+struct ModeOperand {
+  Unfolding u;
+  const float* f32 = nullptr;
+  const __nv_bfloat16* hi = nullptr;
+  const __nv_bfloat16* lo = nullptr;
+};
+
+int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int mode,
+                 int precision, int slot_index, ModeOperand* op) {
+  op->u = make_unfolding(ndim, shape, mode);
+  const Unfolding& u = op->u;
+  if (precision == TSR_PREC_BF16X3) {
+    void *hi, *lo;
+    TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + slot_index, 2 * u.rows * u.ld, &hi));
+    TSR_TRY(slot_get(ctx, SLOT_UNFOLD_LO + slot_index, 2 * u.rows * u.ld, &lo));
+    TSR_TRY(launch_unfold_bf16x2(ctx, dX, shape, u, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo));
+    op->hi = (const __nv_bfloat16*)hi;
+    op->lo = (const __nv_bfloat16*)lo;
+    return TSR_OK;
+  }
+  // mode 0 of a row-major tensor is already its unfolding when rows are aligned
+  if (mode == 0 && u.ld == u.cols) {
+    op->f32 = dX;
+    return TSR_OK;
+  }
+  void* p;
+  TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + slot_index, sizeof(float) * u.rows * u.ld, &p));
+  TSR_TRY(launch_unfold_f32(ctx, dX, shape, u, (float*)p));
+  op->f32 = (const float*)p;
+  return TSR_OK;
+}
+
+// Split-K partial MTTKRP of one mode into `partials` (allocated here).
+int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& ft, int R,
+                        int precision, float** partials, int* splits) {
+  KRSpec kr = make_krspec(op.u, ft, R);
+  SplitPlan plan;
+  bool tc = precision == TSR_PREC_BF16X3;
+  if (tc && !tc_supported(op.u, R))
+    return fail(TSR_E_UNSUPPORTED, "BF16X3 path needs rank <= 256 (got %d)", R);
+  plan = tc ? plan_tc(ctx, op.u.rows, op.u.cols, R) : plan_simt(ctx, op.u.rows, op.u.cols, R);
+  void* p;
+  TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * partial_floats(plan, op.u.rows, R), &p));
+  if (tc)
+    TSR_TRY(launch_mttkrp_tc(ctx, op.hi, op.lo, op.u, kr, plan, (float*)p));
+  else
+    TSR_TRY(launch_mttkrp_simt(ctx, op.f32, op.u, kr, plan, (float*)p));
+  *partials = (float*)p;
+  *splits = plan.splits;
+  return TSR_OK;
+}
+
+int check_precision(int precision) {
+  if (precision != TSR_PREC_FP32 && precision != TSR_PREC_BF16X3)
+    return fail(TSR_E_INVALID_ARG, "unknown precision %d", precision);
+  return TSR_OK;
+}
+
+// Device MTTKRP for one mode into d_out (I_mode x R).
+int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
+                  const FactorTable& ft, int R, int mode, int precision, float* d_out) {
+  ModeOperand op;
+  TSR_TRY(prepare_mode(ctx, dX, ndim, shape, mode, precision, 0, &op));
+  float* partials;
+  int splits;
+  TSR_TRY(run_mttkrp_partials(ctx, op, ft, R, precision, &partials, &splits));
+  TSR_TRY(launch_mttkrp_reduce(ctx, partials, splits, op.u.rows * R, d_out));
+  return TSR_OK;
+}
+
+int upload_factors(tsr_ctx* ctx, int ndim, const int64_t* shape, const float* const* factors,
+                   int64_t R, FactorTable* ft) {
+  int64_t total = 0;
+  for (int m = 0; m < ndim; ++m) total += shape[m] * R;
+  void* d;
+  TSR_TRY(slot_get(ctx, SLOT_FACTORS, sizeof(float) * total, &d));
+  float* p = (float*)d;
+  for (int m = 0; m < ndim; ++m) {
+    TSR_CUDA(cudaMemcpyAsync(p, factors[m], sizeof(float) * shape[m] * R, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    ft->ptr[m] = p;
+    ft->rows[m] = shape[m];
+    p += shape[m] * R;
+  }
+  return TSR_OK;
+}
+
+// SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform.
+uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
+  const uint64_t golden = 0x9E3779B97F4A7C15ull;
+  uint64_t key = mix64(seed * 0x100000001B3ull + stream * 0x2545F4914F6CDD1Dull + golden);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t r = mix64(key + (uint64_t)i * golden);
+    out[i] = (float)((double)(r >> 11) * (1.0 / 9007199254740992.0));
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// CP-ALS driver (cp/core.rs:91-214) on a device-resident tensor.
+// ---------------------------------------------------------------------------
+int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int64_t rank,
+                  int max_iters, double tol, const float* d_init, int precision,
+                  double time_limit_s, float* d_out, tsr_cp_info* info) {
+  auto t_start = std::chrono::steady_clock::now();
+  // core.rs:115-127
+  if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  for (int d = 0; d < ndim; ++d)
+    if (rank > shape[d]) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  if (!(tol >= 0.0 && tol < 1.0)) return fail(TSR_E_INVALID_TOL, "Invalid tolerance: %g", tol);
+  TSR_TRY(check_precision(precision));
+  if (ndim > kMaxModes)
+    return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", ndim, kMaxModes);
+  if (rank > kMaxRank)
+    return fail(TSR_E_UNSUPPORTED, "rank %lld exceeds the supported %d", (long long)rank,
+                kMaxRank);
+  if (ndim < 2 && max_iters > 0)
+    return fail(TSR_E_SHAPE, "Shape mismatch: Need at least 2 factor matrices for MTTKRP");
+  const int R = (int)rank;
+  const int64_t n = numel(ndim, shape);
+
+  // factors live in d_out for the whole run (updated in place)
+  int64_t ftotal = 0;
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_out + ftotal;
+    ft.rows[m] = shape[m];
+    ftotal += shape[m] * R;
+  }
+  if (d_init != d_out)
+    TSR_CUDA(cudaMemcpyAsync(d_out, d_init, sizeof(float) * ftotal, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+
+  // state + FP64 buffers
+  const int hist_n = std::max(max_iters, 1);
+  size_t gbytes = sizeof(double) * (size_t)(2 * ndim + 1) * R * R;
+  size_t sbytes = 256 + sizeof(double) * hist_n;
+  void *gp, *sp;
+  TSR_TRY(slot_get(ctx, SLOT_GRAMS, gbytes, &gp));
+  TSR_TRY(slot_get(ctx, SLOT_STATE, sbytes, &sp));
+  AlsBuffers b;
+  b.grams = (double*)gp;
+  b.hadam = b.grams + (size_t)ndim * R * R;
+  b.ginv = b.hadam + (size_t)ndim * R * R;
+  b.state = (AlsState*)sp;
+  b.history = (double*)((char*)sp + 256);
+  TSR_CUDA(cudaMemsetAsync(sp, 0, sbytes, ctx->stream));
+
+  // per-mode unfoldings, resident for the whole run (the reference re-unfolds
+  // in every mttkrp call, mttkrp.rs:126)
+  std::vector<ModeOperand> ops(ndim);
+  if (max_iters > 0)
+    for (int m = 0; m < ndim; ++m)
+      TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
+  TSR_TRY(launch_norm_sq(ctx, dX, n, b.state));
+  for (int m = 0; m < ndim; ++m)
+    TSR_TRY(launch_gram(ctx, ft.ptr[m], shape[m], R, b.grams + (size_t)m * R * R));
+
+  const float ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
+  bool time_limited = time_limit_s >= 0.0;
+  bool stopped_by_time = false;
+  for (int iter = 0; iter < max_iters; ++iter) {
+    if (time_limited) {
+      AlsState hs;
+      TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (hs.done) break;
+      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+      if (el > time_limit_s) {
+        stopped_by_time = true;
+        break;
+      }
+    }
+    for (int mode = 0; mode < ndim; ++mode) {
+      bool last = mode == ndim - 1;
+      float* partials;
+      int splits;
+      TSR_TRY(run_mttkrp_partials(ctx, ops[mode], ft, R, precision, &partials, &splits));
+      TSR_TRY(launch_chol(ctx, b, ndim, mode, R, ridge, last));
+      TSR_TRY(launch_solve(ctx, b, partials, splits, shape[mode], R, const_cast<float*>(ft.ptr[mode]), mode,
+                               last));
+    }
+    TSR_TRY(launch_fit(ctx, b, ndim, R, tol));
+  }
+  AlsState hs;
+  TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (hs.status & DS_NOT_SPD)
+    return fail(TSR_E_NOT_SPD,
+                "Linear algebra error: Gram matrix is not positive definite (ridge %g also "
+                "failed)", (double)ridge);
+  if (info) {
+    info->fit = hs.fit;
+    info->iters = hs.iter;
+    info->reason = stopped_by_time ? TSR_REASON_TIME_LIMIT
+                   : hs.done       ? hs.reason
+                                   : TSR_REASON_MAX_ITERATIONS;
+    info->oscillation_count = hs.osc;
+    info->oscillated = hs.osc > 0;
+    info->final_fit_change = hs.final_change;
+    info->ridge_used = hs.ridge_used;
+    if (info->fit_history && hs.iter > 0)
+      TSR_CUDA(cudaMemcpy(info->fit_history, b.history, sizeof(double) * hs.iter,
+                          cudaMemcpyDeviceToHost));
+  }
+  return TSR_OK;
+}
+
+}  // namespace tsr
+
+using namespace tsr;
+
+extern "C" {
+
+int tsr_khatri_rao_f32(tsr_ctx* ctx, const float* a, int64_t I, int64_t Ka, const float* b,
+                       int64_t J, int64_t Kb, float* out) {
+  if (Ka != Kb)
+    return fail(TSR_E_COLS_MISMATCH,
+                "Number of columns must match: A has %lld columns, B has %lld columns",
+                (long long)Ka, (long long)Kb);
+  TSR_TRY(check_ctx(ctx));
+  if (I * J * Ka == 0) return TSR_OK;
+  void *da, *db, *dc;
+  TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * I * Ka, &da));
+  TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * J * Ka, &db));
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * I * J * Ka, &dc));
+  TSR_CUDA(cudaMemcpyAsync(da, a, sizeof(float) * I * Ka, cudaMemcpyHostToDevice, ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(db, b, sizeof(float) * J * Ka, cudaMemcpyHostToDevice, ctx->stream));
+  TSR_TRY(launch_khatri_rao(ctx, (const float*)da, I, (const float*)db, J, Ka, (float*)dc));
+  TSR_CUDA(cudaMemcpyAsync(out, dc, sizeof(float) * I * J * Ka, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int tsr_mttkrp_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                   const int64_t* strides, const float* const* factors, int n_factors,
+                   const int64_t* factor_rows, const int64_t* factor_cols, int mode,
+                   int precision, float* out) {
+  if (!shape || (n_factors > 0 && (!factors || !factor_rows || !factor_cols)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(validate_mttkrp(ndim, shape, n_factors, factor_rows, factor_cols, mode));
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  const int R = (int)factor_cols[0];
+  const int64_t nout = shape[mode] * R;
+  if (nout == 0) return TSR_OK;
+  if (numel(ndim, shape) == 0 || R == 0) {
+    std::memset(out, 0, sizeof(float) * nout);
+    return TSR_OK;
+  }
+  float* dX;
+  TSR_TRY(upload_tensor(ctx, tensor, ndim, shape, strides, &dX));
+  FactorTable ft{};
+  TSR_TRY(upload_factors(ctx, ndim, shape, factors, R, &ft));
+  void* dout;
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * nout, &dout));
+  TSR_TRY(mttkrp_device(ctx, dX, ndim, shape, ft, R, mode, precision, (float*)dout));
+  TSR_CUDA(cudaMemcpyAsync(out, dout, sizeof(float) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int tsr_mttkrp_blocked_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                           const int64_t* strides, const float* const* factors, int n_factors,
+                           const int64_t* factor_rows, const int64_t* factor_cols, int mode,
+                           int64_t tile_size, int precision, float* out) {
+  if (tile_size <= 0) return fail(TSR_E_TILE_SIZE, "Tile size must be greater than 0");
+  return tsr_mttkrp_f32(ctx, tensor, ndim, shape, strides, factors, n_factors, factor_rows,
+                        factor_cols, mode, precision, out);
+}
+
+int tsr_mttkrp_all_modes_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                             const float* const* factors, int64_t rank, int precision,
+                             float* const* out) {
+  if (!shape || !factors || !out) return fail(TSR_E_INVALID_ARG, "null argument");
+  std::vector<int64_t> cols(ndim, rank);
+  TSR_TRY(validate_mttkrp(ndim, shape, ndim, shape, cols.data(), 0));
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  const int R = (int)rank;
+  float* dX;
+  TSR_TRY(upload_tensor(ctx, tensor, ndim, shape, nullptr, &dX));
+  FactorTable ft{};
+  TSR_TRY(upload_factors(ctx, ndim, shape, factors, R, &ft));
+  for (int m = 0; m < ndim; ++m) {
+    void* dout;
+    TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * shape[m] * R, &dout));
+    TSR_TRY(mttkrp_device(ctx, dX, ndim, shape, ft, R, m, precision, (float*)dout));
+    TSR_CUDA(cudaMemcpyAsync(out[m], dout, sizeof(float) * shape[m] * R, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return TSR_OK;
+}
+
+int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                       const float* const* d_factors, int64_t rank, int mode, int precision,
+                       float* d_out) {
+  if (!shape || !d_factors || !d_tensor || !d_out) return fail(TSR_E_INVALID_ARG, "null argument");
+  std::vector<int64_t> cols(ndim, rank);
+  TSR_TRY(validate_mttkrp(ndim, shape, ndim, shape, cols.data(), mode));
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = shape[m];
+  }
+  return mttkrp_device(ctx, d_tensor, ndim, shape, ft, (int)rank, mode, precision, d_out);
+}
+
+int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                       int64_t rank, int max_iters, double tol, const float* d_init,
+                       int precision, double time_limit_s, float* d_out_factors,
+                       tsr_cp_info* info) {
+  if (!shape || !d_tensor || !d_init || !d_out_factors)
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(check_ctx(ctx));
+  return cp_als_device(ctx, d_tensor, ndim, shape, rank, max_iters, tol, d_init, precision,
+                       time_limit_s, d_out_factors, info);
+}
+
+int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                   int64_t rank, int max_iters, double tol, const float* init_factors,
+                   uint64_t seed, int precision, double time_limit_s, float* out_factors,
+                   tsr_cp_info* info) {
+  if (!shape || !tensor || !out_factors) return fail(TSR_E_INVALID_ARG, "null argument");
+  if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  for (int d = 0; d < ndim; ++d)
+    if (rank > shape[d]) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  if (!(tol >= 0.0 && tol < 1.0)) return fail(TSR_E_INVALID_TOL, "Invalid tolerance: %g", tol);
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  int64_t ftotal = 0;
+  for (int m = 0; m < ndim; ++m) ftotal += shape[m] * rank;
+  std::vector<float> init_buf;
+  const float* init = init_factors;
+  if (!init) {  // InitStrategy::Random from the library's seeded stream
+    init_buf.resize(ftotal);
+    int64_t off = 0;
+    for (int m = 0; m < ndim; ++m) {
+      seeded_uniform(seed, 200 + m, shape[m] * rank, init_buf.data() + off);
+      off += shape[m] * rank;
+    }
+    init = init_buf.data();
+  }
+  float* dX;
+  TSR_TRY(upload_tensor(ctx, tensor, ndim, shape, nullptr, &dX));
+  void* df;
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * ftotal, &df));
+  TSR_CUDA(cudaMemcpyAsync(df, init, sizeof(float) * ftotal, cudaMemcpyHostToDevice, ctx->stream));
+  TSR_TRY(cp_als_device(ctx, dX, ndim, shape, rank, max_iters, tol, (const float*)df, precision,
+                        time_limit_s, (float*)df, info));
+  TSR_CUDA(cudaMemcpyAsync(out_factors, df, sizeof(float) * ftotal, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,35 @@
+// Host-side entry points of the dense MTTKRP kernels (split-K partials).
+#pragma once
+#include "kr.cuh"
+
+namespace tsr {
+
+struct SplitPlan {
+  int splits = 1;
+  int64_t k_per_split = 0;
+};
+
+// FP32 SIMT kernel (mttkrp_simt.cu).
+SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
+int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
+                       const SplitPlan& plan, float* partials);
+int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out);
+
+// BF16x3 tcgen05 kernel (mttkrp_tc.cu). The unfolding halves hi/lo are bf16
+// with row stride u.ld (a multiple of 8 elements, 16 bytes).
+bool tc_supported(const Unfolding& u, int R);
+SplitPlan plan_tc(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
+int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16* lo,
+                     const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
+                     float* partials);
+
+// Materialised two-factor Khatri-Rao product (the public khatri_rao API).
+int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, int64_t J,
+                      int64_t K, float* C);
+
+// Partial buffer size in floats for a plan.
+inline size_t partial_floats(const SplitPlan& p, int64_t rows, int R) {
+  return (size_t)p.splits * rows * R;
+}
+
+}  // namespace tsr

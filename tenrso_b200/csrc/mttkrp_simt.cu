@@ -1,0 +1,210 @@
+// Dense MTTKRP, FP32 SIMT path: M = X_(n) . KR with the unfolding X_(n)
+// (I_n x K, row stride ld) resident in HBM and the KR rows generated into
+// shared memory per K-step. Split-K over the grid: each CTA owns a K range
+// and writes a partial I_n x R tile; the partials are summed in a fixed order
+// (deterministic) by the consumer (the ALS solve, or mttkrp_reduce_kernel).
+//
+// Replaces the i/r/j triple loop of crates/tenrso-kernels/src/mttkrp.rs:135-143
+// (same sum, different association: per-split partial sums, then a sum over
+// splits).
+#include "kr.cuh"
+#include "mttkrp.cuh"
+
+namespace tsr {
+
+namespace {
+constexpr int BM = 128, BN = 64, BK = 32, NT = 256;
+
+__global__ void __launch_bounds__(NT, 2)
+mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, int64_t ld,
+                         KRSpec kr, int64_t k_per_split, float* __restrict__ partials) {
+  extern __shared__ __align__(16) float simt_smem[];
+  float(*As)[BK][BM + 4] = reinterpret_cast<float(*)[BK][BM + 4]>(simt_smem);
+  float(*Bs)[BK][BN] = reinterpret_cast<float(*)[BK][BN]>(simt_smem + 2 * BK * (BM + 4));
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  const int64_t m0 = (int64_t)blockIdx.y * BM;
+  const int n0 = blockIdx.z * BN;
+  const int R = kr.R;
+  const int64_t kbeg = (int64_t)blockIdx.x * k_per_split;
+  const int64_t kend = min(K, kbeg + k_per_split);
+  const int nsteps = (int)((kend - kbeg + BK - 1) / BK);
+
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+
+  float4 areg[4];
+  float breg[8];
+  // A-tile mapping: 8 threads per row (32 floats = 128 B), 32 rows per pass.
+  auto load_a = [&](int64_t k0) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      int idx = it * NT + tid;
+      int m = idx / 8, kq = idx % 8;
+      int64_t gm = m0 + m, gk = k0 + kq * 4;
+      if (gm < rows && gk < kend)
+        areg[it] = __ldg(reinterpret_cast<const float4*>(A + gm * ld + gk));
+      else
+        areg[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+      // columns past kend inside the same float4 belong to the next split
+      if (gm < rows && gk < kend && gk + 4 > kend) {
+        float* p = reinterpret_cast<float*>(&areg[it]);
+        for (int e = (int)(kend - gk); e < 4; ++e) p[e] = 0.f;
+      }
+    }
+  };
+  auto store_a = [&](int buf) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      int idx = it * NT + tid;
+      int m = idx / 8, kq = idx % 8;
+      As[buf][kq * 4 + 0][m] = areg[it].x;
+      As[buf][kq * 4 + 1][m] = areg[it].y;
+      As[buf][kq * 4 + 2][m] = areg[it].z;
+      As[buf][kq * 4 + 3][m] = areg[it].w;
+    }
+  };
+  // B-tile mapping: thread -> (kk = tid / 8, 8 consecutive columns).
+  auto gen_b = [&](int64_t k0) {
+    int kk = tid / 8, c0 = (tid % 8) * 8;
+    int64_t j = k0 + kk;
+    if (j < kend) {
+      uint32_t off[kMaxModes];
+      kr_row_offsets(kr, (uint32_t)j, off);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        int c = n0 + c0 + e;
+        breg[e] = (c < R) ? kr_value(kr, off, c) : 0.f;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) breg[e] = 0.f;
+    }
+  };
+  auto store_b = [&](int buf) {
+    int kk = tid / 8, c0 = (tid % 8) * 8;
+    *reinterpret_cast<float4*>(&Bs[buf][kk][c0]) = make_float4(breg[0], breg[1], breg[2], breg[3]);
+    *reinterpret_cast<float4*>(&Bs[buf][kk][c0 + 4]) =
+        make_float4(breg[4], breg[5], breg[6], breg[7]);
+  };
+
+  if (nsteps > 0) {
+    load_a(kbeg);
+    gen_b(kbeg);
+    store_a(0);
+    store_b(0);
+  }
+  __syncthreads();
+  for (int s = 0; s < nsteps; ++s) {
+    const int buf = s & 1;
+    const bool more = s + 1 < nsteps;
+    if (more) {
+      load_a(kbeg + (int64_t)(s + 1) * BK);
+      gen_b(kbeg + (int64_t)(s + 1) * BK);
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 8]);
+      float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 8 + 4]);
+      float4 b = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+      float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    if (more) {
+      store_a(buf ^ 1);
+      store_b(buf ^ 1);
+    }
+    __syncthreads();
+  }
+
+  float* P = partials + (int64_t)blockIdx.x * rows * R;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int64_t gm = m0 + ty * 8 + i;
+    if (gm >= rows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int c = n0 + tx * 4 + j;
+      if (c < R) P[gm * R + c] = acc[i][j];
+    }
+  }
+}
+
+__global__ void mttkrp_reduce_kernel(const float* __restrict__ partials, int splits, int64_t n,
+                                     float* __restrict__ out) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double s = 0.0;
+  for (int p = 0; p < splits; ++p) s += (double)__ldg(partials + (int64_t)p * n + k);
+  out[k] = (float)s;
+}
+// khatri_rao.rs:56-89: C[a*J + b, k] = A[a, k] * B[b, k].
+__global__ void khatri_rao_kernel(const float* __restrict__ A, int64_t I,
+                                  const float* __restrict__ B, int64_t J, int64_t K,
+                                  float* __restrict__ C) {
+  int64_t n = I * J * K;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t k = e % K, row = e / K;
+    int64_t a = row / J, b = row % J;
+    C[e] = __ldg(A + a * K + k) * __ldg(B + b * K + k);
+  }
+}
+}  // namespace
+
+int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, int64_t J,
+                      int64_t K, float* C) {
+  int64_t n = I * J * K;
+  unsigned grid = (unsigned)std::min<int64_t>(ceil_div(n, 256), (int64_t)ctx->sm_count * 8);
+  khatri_rao_kernel<<<grid, 256, 0, ctx->stream>>>(A, I, B, J, K, C);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
+  SplitPlan p;
+  int64_t mt = ceil_div(rows, BM), nt = ceil_div(R, BN);
+  int64_t want = std::max<int64_t>(1, (int64_t)ctx->sm_count * 3 / (mt * nt));
+  int64_t steps = ceil_div(K, BK);
+  want = std::min<int64_t>(want, steps);
+  p.k_per_split = round_up(ceil_div(K, want), BK);
+  p.splits = (int)ceil_div(K, p.k_per_split);
+  return p;
+}
+
+int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
+                       const SplitPlan& plan, float* partials) {
+  if (u.cols >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "unfolding too wide");
+  dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, BM), (unsigned)ceil_div(kr.R, BN));
+  if (grid.y > 65535 || grid.z > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
+  const size_t smem = sizeof(float) * 2 * BK * (BM + 4 + BN);
+  static bool attr = false;
+  if (!attr) {
+    TSR_CUDA(cudaFuncSetAttribute(mttkrp_f32_splitk_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  mttkrp_f32_splitk_kernel<<<grid, NT, smem, ctx->stream>>>(A, u.rows, u.cols, u.ld, kr,
+                                                            plan.k_per_split, partials);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out) {
+  mttkrp_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, ctx->stream>>>(partials, splits, n,
+                                                                            out);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+}  // namespace tsr

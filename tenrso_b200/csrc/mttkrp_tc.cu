@@ -1,0 +1,381 @@
+// Dense MTTKRP, BF16x3 tensor-core path (sm_100a tcgen05).
+//
+// M = X_(n) . KR computed as  Xhi.KRhi + Xhi.KRlo + Xlo.KRhi  where x = hi + lo
+// is an exact-to-2^-16 split of each fp32 value into two bf16 values; the
+// three bf16 MMAs accumulate in fp32 in tensor memory (TMEM). The lo.lo term
+// (relative size 2^-16 * 2^-16) is dropped.
+//
+// Per CTA: one 128-row M tile of the unfolding and one K range (split-K).
+//   warp 0      TMA producer: X_(n) hi/lo tiles (128 x 64 bf16, 128-byte
+//               swizzle) into a ring of shared-memory stages.
+//   warp 1      TMEM allocator and the single MMA-issuing thread.
+//   warps 2..5  Khatri-Rao producers: form 64 KR rows per stage from the other
+//               factors (kr.cuh), split them into bf16 hi/lo and write them as
+//               the K-major B operand (N = R padded to 16) in the same
+//               swizzled layout; afterwards the epilogue (TMEM -> registers ->
+//               split-K partials in HBM).
+// KR rows are never written to global memory. Every mbarrier wait is bounded;
+// a wait that runs out raises DS_TIMEOUT in the status word and the CTA
+// drains and exits (TMA copies waited for, TMEM freed).
+//
+// Replaces the hot loop of crates/tenrso-kernels/src/mttkrp.rs:135-143 (and
+// the KR materialisation of mttkrp.rs:182-240) for the mixed-precision mode.
+#include "mttkrp.cuh"
+#include "sm100.cuh"
+
+namespace tsr {
+
+namespace {
+
+constexpr int TC_BM = 128;   // M tile (TMEM lanes)
+constexpr int TC_BK = 64;    // K per stage: one 128-byte swizzle row of bf16
+constexpr int TC_THREADS = 192;
+constexpr int A_TILE_BYTES = TC_BM * TC_BK * 2;  // 16 KB
+constexpr long long WAIT_BUDGET = 1ll << 31;     // ~1 s at B200 clocks
+
+struct TcParams {
+  int64_t rows;
+  int64_t K;
+  int64_t k_per_split;
+  int n_pad;
+  int stages;
+  int tmem_cols;
+  KRSpec kr;
+  float* partials;
+  unsigned* status;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+template <bool VEC4>
+__device__ __forceinline__ void kr_produce_stage(const TcParams& p, uint8_t* b_hi, uint8_t* b_lo,
+                                                 int64_t kbase, int64_t kend, int t) {
+  const int kq = t & 7;   // which 8-wide k chunk of the 64-wide stage
+  const int ng = t >> 3;  // 16 groups of 4 columns per 64-column pass
+  const KRSpec& kr = p.kr;
+  const int R = kr.R;
+  uint32_t off[8][kMaxModes];
+  bool valid[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int64_t j = kbase + kq * 8 + e;
+    valid[e] = j < kend;
+    if (valid[e]) kr_row_offsets(kr, (uint32_t)j, off[e]);
+  }
+  for (int nb = 0; nb < p.n_pad; nb += 64) {
+    const int n0 = nb + ng * 4;
+    if (n0 >= p.n_pad) break;
+    float v[8][4];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      if (!valid[e] || n0 >= R) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[e][c] = 0.f;
+        continue;
+      }
+      if (VEC4) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(kr.f[0] + off[e][0] + n0));
+        v[e][0] = a.x; v[e][1] = a.y; v[e][2] = a.z; v[e][3] = a.w;
+#pragma unroll
+        for (int q = 1; q < kMaxModes; ++q) {
+          if (q < kr.n_other) {
+            float4 b = __ldg(reinterpret_cast<const float4*>(kr.f[q] + off[e][q] + n0));
+            v[e][0] *= b.x; v[e][1] *= b.y; v[e][2] *= b.z; v[e][3] *= b.w;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[e][c] = (n0 + c < R) ? kr_value(kr, off[e], n0 + c) : 0.f;
+      }
+    }
+    // swizzled K-major store: row n, 16-byte chunk kq ^ (n & 7)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int n = n0 + c;
+      float h[8], l[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        __nv_bfloat16 hb = __float2bfloat16_rn(v[e][c]);
+        h[e] = __bfloat162float(hb);
+        l[e] = v[e][c] - h[e];
+      }
+      uint4 hv = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]),
+                            pack_bf16x2(h[4], h[5]), pack_bf16x2(h[6], h[7]));
+      uint4 lv = make_uint4(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]),
+                            pack_bf16x2(l[4], l[5]), pack_bf16x2(l[6], l[7]));
+      const uint32_t byte = (uint32_t)n * 128u + ((uint32_t)(kq ^ (n & 7)) << 4);
+      *reinterpret_cast<uint4*>(b_hi + byte) = hv;
+      *reinterpret_cast<uint4*>(b_lo + byte) = lv;
+    }
+  }
+}
+
+template <bool VEC4>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
+                     const __grid_constant__ CUtensorMap map_lo, TcParams p) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  // 1024-byte alignment for the swizzled tiles
+  uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+  const int S = p.stages;
+  const uint32_t b_bytes = (uint32_t)p.n_pad * 128u;
+  const uint32_t stage_bytes = 2u * A_TILE_BYTES + 2u * b_bytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
+  uint64_t* tma_full = bars;
+  uint64_t* kr_full = bars + S;
+  uint64_t* empty = bars + 2 * S;
+  uint64_t* done = bars + 3 * S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t m0 = (int64_t)blockIdx.y * TC_BM;
+  const int64_t kbeg = (int64_t)blockIdx.x * p.k_per_split;
+  const int64_t kend = min(p.K, kbeg + p.k_per_split);
+  const int nsteps = kend > kbeg ? (int)((kend - kbeg + TC_BK - 1) / TC_BK) : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&tma_full[s], 1);
+      mbar_init(&kr_full[s], 4);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    prefetch_tmap(&map_hi);
+    prefetch_tmap(&map_lo);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, (uint32_t)p.tmem_cols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  auto stage_ptr = [&](int s) { return smem + (size_t)s * stage_bytes; };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued_upto = 0;
+      for (int it = 0; it < nsteps; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, WAIT_BUDGET)) {
+          *abort_flag = 1;
+          atomicOr(p.status, DS_TIMEOUT);
+          break;
+        }
+        uint8_t* st = stage_ptr(s);
+        mbar_arrive_expect_tx(&tma_full[s], 2u * A_TILE_BYTES);
+        const int32_t x = (int32_t)(kbeg + (int64_t)it * TC_BK);
+        const int32_t y = (int32_t)m0;
+        tma_load_2d(st, &map_hi, x, y, &tma_full[s]);
+        tma_load_2d(st + A_TILE_BYTES, &map_lo, x, y, &tma_full[s]);
+        issued_upto = it + 1;
+      }
+      // drain: the last issued phase of every stage must have landed before
+      // the CTA may exit (bounded; no abort short-cut here)
+      for (int it = issued_upto - S > 0 ? issued_upto - S : 0; it < issued_upto; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        long long t0 = clock64();
+        while (!mbar_try_wait(&tma_full[s], ph) && clock64() - t0 < WAIT_BUDGET) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(TC_BM, p.n_pad);
+      for (int it = 0; it < nsteps; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!mbar_wait(&tma_full[s], ph, abort_flag, WAIT_BUDGET) ||
+            !mbar_wait(&kr_full[s], ph, abort_flag, WAIT_BUDGET)) {
+          *abort_flag = 1;
+          atomicOr(p.status, DS_TIMEOUT);
+          break;
+        }
+        tc_fence_after();
+        uint8_t* st = stage_ptr(s);
+        const uint32_t a_hi = smem_u32(st), a_lo = a_hi + A_TILE_BYTES;
+        const uint32_t b_hi = a_hi + 2 * A_TILE_BYTES, b_lo = b_hi + b_bytes;
+#pragma unroll
+        for (int kk = 0; kk < TC_BK / 16; ++kk) {
+          const uint32_t koff = kk * 32;  // 16 bf16 = 32 bytes along K
+          const uint64_t dah = desc_sw128_kmajor(a_hi + koff);
+          const uint64_t dal = desc_sw128_kmajor(a_lo + koff);
+          const uint64_t dbh = desc_sw128_kmajor(b_hi + koff);
+          const uint64_t dbl = desc_sw128_kmajor(b_lo + koff);
+          mma_bf16(tmem, dah, dbh, idesc, (it > 0 || kk > 0) ? 1u : 0u);
+          mma_bf16(tmem, dah, dbl, idesc, 1u);
+          mma_bf16(tmem, dal, dbh, idesc, 1u);
+        }
+        mma_commit(&empty[s]);
+      }
+      mma_commit(done);  // tracks every MMA issued above (also on abort)
+    }
+  } else {
+    // Khatri-Rao producers (warps 2..5, 128 threads)
+    const int t = threadIdx.x - 64;
+    for (int it = 0; it < nsteps; ++it) {
+      const int s = it % S;
+      const uint32_t ph = (uint32_t)(it / S) & 1u;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, abort_flag, WAIT_BUDGET) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) {
+          *abort_flag = 1;
+          atomicOr(p.status, DS_TIMEOUT);
+        }
+        break;
+      }
+      uint8_t* st = stage_ptr(s);
+      kr_produce_stage<VEC4>(p, st + 2 * A_TILE_BYTES, st + 2 * A_TILE_BYTES + b_bytes,
+                             kbeg + (int64_t)it * TC_BK, kend, t);
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&kr_full[s]);
+    }
+    // epilogue: TMEM accumulator -> split-K partial rows
+    int ok = 1;
+    if (lane == 0) ok = mbar_wait(done, 0, abort_flag, WAIT_BUDGET) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    tc_fence_after();
+    const int q = warp & 3;  // TMEM lane quadrant this warp may access
+    const int64_t row = m0 + q * 32 + lane;
+    const int R = p.kr.R;
+    float* out = p.partials + (int64_t)blockIdx.x * p.rows * R + row * R;
+    if (ok && nsteps > 0) {
+      for (int c0 = 0; c0 < p.n_pad; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        if (row < p.rows) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (c0 + i < R) out[c0 + i] = v[i];
+        }
+      }
+    } else if (row < p.rows) {
+      if (!ok && lane == 0) atomicOr(p.status, DS_TIMEOUT);
+      for (int c = 0; c < R; ++c) out[c] = 0.f;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, (uint32_t)p.tmem_cols);
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+int make_map(CUtensorMap* map, const __nv_bfloat16* base, int64_t rows, int64_t cols,
+             int64_t ld) {
+  EncodeTiledFn enc = get_encode();
+  if (!enc) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (((uintptr_t)base & 15) || (ld * 2) % 16)
+    return fail(TSR_E_INVALID_ARG, "TMA operand misaligned");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)TC_BM};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TSR_OK;
+}
+
+int n_pad_of(int R) { return (int)round_up(R, 16); }
+
+int stages_for(int n_pad) {
+  int stage = 2 * A_TILE_BYTES + 2 * n_pad * 128;
+  int s = (200 * 1024) / stage;
+  return s > 4 ? 4 : s;
+}
+
+}  // namespace
+
+bool tc_supported(const Unfolding& u, int R) {
+  return R >= 1 && n_pad_of(R) <= 256 && u.cols < (int64_t)INT32_MAX && u.rows < INT32_MAX;
+}
+
+SplitPlan plan_tc(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
+  (void)R;
+  SplitPlan p;
+  int64_t mt = ceil_div(rows, TC_BM);
+  int64_t steps = ceil_div(K, TC_BK);
+  int64_t want = std::max<int64_t>(1, ctx->sm_count / mt);
+  want = std::min<int64_t>(want, steps);
+  int64_t steps_per = ceil_div(steps, want);
+  p.k_per_split = steps_per * TC_BK;
+  p.splits = (int)ceil_div(K, p.k_per_split);
+  return p;
+}
+
+int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16* lo,
+                     const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
+                     float* partials) {
+  if (!tc_supported(u, kr.R)) return fail(TSR_E_UNSUPPORTED, "BF16X3 MTTKRP: rank too large");
+  CUtensorMap mh, ml;
+  TSR_TRY(make_map(&mh, hi, u.rows, u.cols, u.ld));
+  TSR_TRY(make_map(&ml, lo, u.rows, u.cols, u.ld));
+  TcParams p;
+  p.rows = u.rows;
+  p.K = u.cols;
+  p.k_per_split = plan.k_per_split;
+  p.n_pad = n_pad_of(kr.R);
+  p.stages = stages_for(p.n_pad);
+  p.tmem_cols = 32;
+  while (p.tmem_cols < p.n_pad) p.tmem_cols *= 2;
+  p.kr = kr;
+  p.partials = partials;
+  p.status = ctx->d_status;
+  bool vec4 = (kr.R % 4) == 0;
+  for (int q = 0; q < kr.n_other && vec4; ++q) vec4 = ((uintptr_t)kr.f[q] & 15) == 0;
+  size_t stage = 2 * A_TILE_BYTES + 2 * (size_t)p.n_pad * 128;
+  size_t smem = 1024 + (size_t)p.stages * stage + 8 * (3 * p.stages + 1) + 16;
+  dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, TC_BM));
+  if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
+  if (vec4) {
+    TSR_CUDA(cudaFuncSetAttribute(mttkrp_bf16x3_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mttkrp_bf16x3_kernel<true><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
+  } else {
+    TSR_CUDA(cudaFuncSetAttribute(mttkrp_bf16x3_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mttkrp_bf16x3_kernel<false><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
+  }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+}  // namespace tsr

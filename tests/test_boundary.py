@@ -1,0 +1,95 @@
+"""The C-ABI boundary without a GPU: the library loads, exports every symbol
+include/tenrso_b200.h declares, and reproduces tenrso's argument validation
+(messages from mttkrp.rs / khatri_rao.rs / cp/core.rs) before any device
+work. No call here reaches a kernel."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import tenrso_b200 as tb
+from tenrso_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "tenrso_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tsr_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = header_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_version_and_status_strings():
+    lib = _lib.load()
+    assert b"sm_100a" in lib.tsr_version()
+    assert lib.tsr_status_string(0) == b"ok"
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_mttkrp_error_messages(kats, case):
+    k = kats["mttkrp_errors"][case]
+    X = np.ones(k["shape"], dtype=np.float32)
+    fs = [np.array(f, dtype=np.float32) for f in k["factors"]]
+    with pytest.raises(tb.TenrsoError, match=k["expect"]):
+        tb.mttkrp(X, fs, k["mode"])
+
+
+def test_mttkrp_exact_wording():
+    X = np.ones((2, 3), dtype=np.float32)
+    with pytest.raises(tb.TenrsoError) as e:
+        tb.mttkrp(X, [np.ones((2, 1)), np.ones((3, 1))], 5)
+    assert str(e.value) == "Mode 5 out of bounds for tensor with rank 2"
+    with pytest.raises(tb.TenrsoError) as e:
+        tb.mttkrp(X, [np.ones((2, 1)), np.ones((4, 1))], 0)
+    assert str(e.value) == "Factor matrix 1 has 4 rows, expected 3 (tensor mode-1 size)"
+    with pytest.raises(tb.TenrsoError) as e:
+        tb.mttkrp(np.ones(4, np.float32), [np.ones((4, 1))], 0)
+    assert str(e.value) == "Need at least 2 factor matrices for MTTKRP"
+
+
+def test_blocked_tile_size_zero():
+    X = np.ones((2, 3, 4), dtype=np.float32)
+    fs = [np.ones((n, 2), np.float32) for n in X.shape]
+    with pytest.raises(tb.TenrsoError, match="Tile size must be greater than 0"):
+        tb.mttkrp_blocked(X, fs, 0, 0)
+
+
+def test_khatri_rao_column_mismatch(kats):
+    k = kats["khatri_rao_errors"][0]
+    with pytest.raises(tb.TenrsoError, match=k["expect"]):
+        tb.khatri_rao(np.array(k["a"], np.float32), np.array(k["b"], np.float32))
+
+
+def test_cp_als_validation():
+    X = np.ones((3, 4, 5), dtype=np.float32)
+    with pytest.raises(tb.TenrsoError, match="Invalid rank: 0"):
+        tb.cp_als(X, 0, 5, 0.0)
+    with pytest.raises(tb.TenrsoError, match="Invalid rank: 4"):
+        tb.cp_als(X, 4, 5, 0.0)
+    with pytest.raises(tb.TenrsoError, match="Invalid tolerance"):
+        tb.cp_als(X, 2, 5, 1.0)
+    with pytest.raises(tb.TenrsoError, match="Invalid tolerance"):
+        tb.cp_als(X, 2, 5, -0.1)
+
+
+def test_no_cpu_fallback_without_device():
+    """Valid arguments need a device: without one the call fails loudly."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _lib.load()
+    h = C.c_void_p()
+    rc = lib.tsr_ctx_create(0, None, C.byref(h))
+    assert rc == 9  # TSR_E_CUDA
+    assert lib.tsr_last_error()
