@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""CP-ALS benchmark: iterations/s of the mixed-precision (BF16x3 tensor-core
+MTTKRP, FP64 Gram/solve/fit) CP-ALS on a 256^3 rank-64 FP32 tensor, beside
+the plain-FP32 GPU path, with the fits of both.
+
+    python bench.py --gpus N --steps K --warmup W [--impl reference]
+
+One step = one CP-ALS call of 10 iterations (tol 0) on the resident tensor.
+N > 1 runs one independent CP-ALS replica per GPU (weak scaling; the dense
+path has no data exchange between replicas). `--impl reference` times the
+CPU restatement of tenrso's own serial cp_als path instead (rank 0 only).
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CP-ALS iter/s (256^3 R=64; CSF 5e7 nnz) mixed vs FP32 GPU at equal fit"
+SHAPE = (256, 256, 256)
+RANK = 64
+ITERS = 10
+SEED = 0xC2
+WORKLOAD = "dense CP-ALS 256x256x256 rank 64, 10 iterations, tol 0"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_inputs():
+    from tenrso_b200 import synth
+    X, _ = synth.dense_lowrank(SHAPE, RANK, seed=SEED, dist="uniform", noise=0.005)
+    init = synth.init_factors(SHAPE, RANK, SEED)
+    return X, init
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    """The CPU restatement of tenrso's serial cp_als<f32> (oracle/, the
+    reference's own loop order: unfold copy, materialised Khatri-Rao, i/r/j
+    triple loop, per-row solve). One step = one of the four MTTKRP-based
+    updates of an iteration (mode 0 MTTKRP + Gram Hadamard + solve); an
+    iteration is four of them (three modes + the fit's extra MTTKRP)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    X, init = make_inputs()
+    G = orc.gram(init[1]) * orc.gram(init[2])
+
+    def step():
+        M = orc.mttkrp(X, init, 0, faithful=True)
+        orc.solve(M, G)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    it_s = 1.0 / (4.0 * dt)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": it_s, "unit": "iter/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
+        "config": {"workload": WORKLOAD, "sample": "one MTTKRP-based mode update per step"},
+        "cpu_baseline": {"value": it_s, "unit": "iter/s", "cores": 1, "kind": "port",
+                         "sample": "mode-0 MTTKRP + Gram-Hadamard + row solve of the faithful "
+                                   "f32 restatement, x4 per iteration"},
+        "e2e": {"value": it_s, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import tenrso_b200 as tb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = tb.Context(local, stream=stream.cuda_stream)
+
+    X, init = make_inputs()
+    dX = torch.from_numpy(X).cuda()
+    flat_init = np.concatenate([f.ravel() for f in init])
+    dinit = torch.from_numpy(flat_init).cuda()
+    dout = torch.empty_like(dinit)
+    shape = list(SHAPE)
+
+    def step(prec):
+        return tb.cp_als_dev(dX.data_ptr(), shape, RANK, ITERS, 0.0, dinit.data_ptr(),
+                             dout.data_ptr(), prec, ctx=ctx)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        l0 = ctx.launches
+        ev0.record(stream)
+        res = None
+        for _ in range(steps):
+            res = step(prec)
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, res, ctx.launches - l0
+
+    for _ in range(args.warmup):
+        step("bf16x3")
+        step("fp32")
+    # clocks are sampled while the timed work runs; if one timed pass is too
+    # short for the sampler, the same work repeats untimed until ~1.5 s of
+    # load has been sampled
+    sampler = ClockSampler(local)
+    sampler.start()
+    soak_t0 = time.perf_counter()
+    ms_mixed, res_mixed, launches = timed("bf16x3", args.steps)
+    ms_fp32, res_fp32, _ = timed("fp32", args.steps)
+    while time.perf_counter() - soak_t0 < 1.5:
+        step("bf16x3")
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+
+    iters_total = ITERS * args.steps * world
+    value = iters_total / (ms_mixed / 1e3)
+    fp32_value = iters_total / (ms_fp32 / 1e3)
+    fit_mixed, fit_fp32 = res_mixed[0], res_fp32[0]
+
+    # roofline: the dense MTTKRP kernel alone (L2 flushed between launches)
+    d_factors = [dinit.data_ptr() + 4 * sum(SHAPE[:m]) * RANK for m in range(3)]
+    kms = []
+    for mode in range(3):
+        ms, splits = tb.profile_mttkrp_dev(dX.data_ptr(), shape, d_factors, RANK, mode,
+                                           "bf16x3", iters=10, flush_l2=True, ctx=ctx)
+        kms.append(ms)
+    kernel_ms = sum(kms) / len(kms)
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    alg_bytes = 4 * n + 3 * SHAPE[0] * RANK * 4  # fp32 tensor + factors (B_min per MTTKRP)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "mttkrp_bf16x3_kernel", "kernel_ms": kernel_ms,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # e2e through the host API: pinned host tensor in, factors out
+    Xp = torch.from_numpy(X).pin_memory().numpy()
+    initp = [torch.from_numpy(f).pin_memory().numpy() for f in init]
+    tb.cp_als(Xp, RANK, ITERS, 0.0, init=initp, precision="bf16x3", ctx=ctx)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(e2e_steps):
+        tb.cp_als(Xp, RANK, ITERS, 0.0, init=initp, precision="bf16x3", ctx=ctx)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_wall = [e2e_s]
+    if dist is not None:
+        t = torch.tensor(e2e_wall, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": ITERS * world / e2e_s, "unit": "iter/s",
+           "h2d_bytes_per_step": int(X.nbytes + flat_init.nbytes),
+           "d2h_bytes_per_step": int(flat_init.nbytes + 64),
+           "api": "tsr_cp_als_f32 (host pointers)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        G = orc.gram(init[1]) * orc.gram(init[2])
+        t0 = time.perf_counter()
+        M = orc.mttkrp(X, init, 0, faithful=True)
+        orc.solve(M, G)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / (4.0 * dt), "unit": "iter/s", "cores": 1, "kind": "port",
+               "sample": "one mode-0 MTTKRP + Gram-Hadamard + solve of the faithful serial "
+                         "f32 restatement of cp_als on the same tensor, x4 per iteration"}
+
+    if dist is not None:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 MTTKRP (fp32 accumulate) + f64 Gram/solve/fit",
+            "data": "synthetic: seeded rank-64 U(0,1) factors + 0.5% Gaussian noise, fp32",
+            "config": {"workload": WORKLOAD, "shape": list(SHAPE), "rank": RANK,
+                       "iterations_per_step": ITERS, "precision": "bf16x3",
+                       "parallelism": f"replicas{world}" if world > 1 else "1 GPU",
+                       "l2": "working set per step > L2 (X 64 MiB + per-mode unfoldings "
+                             "192 MiB re-written every step)"},
+            "fp32_path": {"value": fp32_value, "unit": "iter/s", "fit": fit_fp32,
+                          "ms_per_step": ms_fp32 / args.steps},
+            "speedup_mixed_vs_fp32": value / fp32_value,
+            "fit_mixed": fit_mixed, "fit_fp32": fit_fp32,
+            "fit_abs_diff": abs(fit_mixed - fit_fp32),
+            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

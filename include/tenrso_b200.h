@@ -118,6 +118,15 @@ int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
                        const float* const* d_factors, int64_t rank, int mode, int precision,
                        float* d_out);
 
+/* Kernel-only timing of the dense MTTKRP (the roofline figure): the unfolding
+ * is prepared once, then `iters` launches of the MTTKRP kernel are timed with
+ * CUDA events on the context's stream, optionally writing a buffer larger
+ * than L2 between launches. No tenrso counterpart (measurement aid). */
+int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
+                               const int64_t* shape, const float* const* d_factors, int64_t rank,
+                               int mode, int precision, int iters, int flush_l2,
+                               double* ms_per_launch, int64_t* splits_out);
+
 /* ---- CP-ALS: crates/tenrso-decomp/src/cp/core.rs:91-214 -----------------
  * Same loop, validation (rank in [1, min I_n], tol in [0,1)), fit, oscillation
  * and convergence rules. init_factors: concatenated row-major I_0xR, I_1xR, ...

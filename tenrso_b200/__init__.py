@@ -20,6 +20,7 @@ from .dense import (  # noqa: F401
     mttkrp_dev,
     mttkrp_fused,
     mttkrp_fused_parallel,
+    profile_mttkrp_dev,
 )
 
 __version__ = "0.1.0"

@@ -1,43 +1,90 @@
 // FP64 kernels of the ALS sweep. Replace, from crates/tenrso-decomp/src/cp/:
-//   compute_gram_hadamard / compute_gram_matrix   helpers.rs:409-452
+//   compute_gram_matrix / compute_gram_hadamard   helpers.rs:409-452
 //   solve_least_squares (per-row lstsq + ridge)   helpers.rs:455-495
 //   compute_norm_squared / compute_fit            helpers.rs:498-579
 //   convergence + oscillation bookkeeping          core.rs:173-198
-// The per-row least-squares solves become one Cholesky factorisation of the
-// symmetric Gram G (FP64), its inverse, and a row-parallel product M . G^-1.
+// The per-row least-squares solves become one in-place Gauss-Jordan inverse of
+// the symmetric Gram G (FP64, no pivoting: every pivot of an SPD matrix is
+// positive, so a non-positive pivot is the "not SPD" signal that triggers the
+// reference's ridge retry) and a row-parallel product M . G^-1.
 // ||Xhat||^2 and <X, Xhat> come from the Grams and the last mode's MTTKRP
 // (mathematically identical to the extra mode-0 MTTKRP of helpers.rs:558-579).
+// Grams are stored as their upper triangle (row a, column c >= a).
 #include "als.cuh"
 
 namespace tsr {
 
 namespace {
 
-__global__ void gram_kernel(const float* __restrict__ U, int64_t rows, int R, int rows_per_cta,
-                            double* __restrict__ gram) {
-  extern __shared__ double sh[];
-  double* Us = sh;  // [rows_per_cta][R]
-  int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
-  int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
-  for (int k = threadIdx.x; k < nr * R; k += blockDim.x) Us[k] = (double)U[r0 * R + k];
-  __syncthreads();
-  for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-    int a = e / R, c = e % R;
-    if (c < a) continue;  // symmetric: compute upper, mirror
-    double s = 0.0;
-    for (int i = 0; i < nr; ++i) s += Us[i * R + a] * Us[i * R + c];
-    atomicAdd(gram + a * R + c, s);
-    if (c != a) atomicAdd(gram + c * R + a, s);
+__device__ __forceinline__ double sym(const double* g, int R, int a, int c) {
+  return a <= c ? g[a * R + c] : g[c * R + a];
+}
+
+// Upper triangle of U^T U accumulated into `gram` (pre-zeroed) with one FP64
+// atomic per entry per CTA. Thread (ty, tx) of a 16 x 16 grid owns entries
+// (ty + 16a, tx + 16b); rows are staged through shared memory in chunks, so a
+// row costs 2*RB shared loads for RB*RB FMAs. Products of fp32 values are
+// exact in FP64.
+template <int RB>
+__global__ void __launch_bounds__(256)
+gram_kernel(const float* __restrict__ U, int64_t rows, int R, int64_t rows_per_cta,
+            double* __restrict__ gram) {
+  constexpr int CH = 32;
+  __shared__ double Us[CH * 16 * RB];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[RB][RB];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = 0.0;
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+  const int64_t r1 = rows < r0 + rows_per_cta ? rows : r0 + rows_per_cta;
+  const int LD = 16 * RB;
+  for (int64_t c0 = r0; c0 < r1; c0 += CH) {
+    const int nr = (int)(r1 - c0 < CH ? r1 - c0 : CH);
+    __syncthreads();
+#pragma unroll 4
+    for (int k = threadIdx.x; k < nr * LD; k += 256) {
+      const int i = k / LD, c = k % LD;
+      Us[k] = c < R ? (double)__ldg(U + (c0 + i) * R + c) : 0.0;
+    }
+    __syncthreads();
+    for (int i = 0; i < nr; ++i) {
+      double x[RB], y[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) x[ai] = Us[i * LD + ty + 16 * ai];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) y[bj] = Us[i * LD + tx + 16 * bj];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) acc[ai][bj] += x[ai] * y[bj];
+    }
   }
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int a = ty + 16 * ai, c = tx + 16 * bj;
+      if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
+    }
 }
 
 __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, AlsState* st) {
-  double s = 0.0;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    double v = X[k];
-    s += v * v;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const int64_t n4 = ((uintptr_t)X & 15) ? 0 : n / 4;
+  const float4* X4 = reinterpret_cast<const float4*>(X);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += stride) {
+    float4 v = __ldg(X4 + k);
+    s0 += (double)v.x * v.x;
+    s1 += (double)v.y * v.y;
+    s2 += (double)v.z * v.z;
+    s3 += (double)v.w * v.w;
   }
+  for (int64_t k = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+    s0 += (double)X[k] * X[k];
+  double s = (s0 + s1) + (s2 + s3);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   __shared__ double ws[32];
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
@@ -49,81 +96,104 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, AlsState*
   }
 }
 
-// Outer-product Cholesky on A (R x R, row-major, shared). One barrier per
-// column: step j subtracts a_ij a_kj / a_jj from the trailing lower triangle.
-// Afterwards L_ij = a_ij / sqrt(a_jj). Returns false (to all threads) if a
-// pivot is not positive or not finite.
-__device__ bool chol_inplace(double* A, int R, int* bad) {
-  if (threadIdx.x == 0) *bad = 0;
-  __syncthreads();
-  for (int j = 0; j < R; ++j) {
-    double d = A[j * R + j];
-    if (!(d > 0.0) || !isfinite(d)) {
-      if (threadIdx.x == 0) *bad = 1;
-      break;  // every thread sees the same d and breaks together
+// Gauss-Jordan inverse of the R x R Hadamard G without pivoting, register
+// blocked: thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns
+// tx + 16b (RB x RB doubles). Each pivot step publishes row k and column k
+// through double-buffered shared vectors (one barrier per step); all updates
+// are register FMAs. An SPD matrix has only positive pivots, so a pivot that
+// is not positive (or not finite) reports "not SPD" (uniformly across the CTA).
+template <int RB>
+__device__ bool gj_inverse_reg(double (&a)[RB][RB], double* prow, double* pcol, int R) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int k = 0; k < R; ++k) {
+    double* rowk = prow + (k & 1) * kMaxRank;
+    double* colk = pcol + (k & 1) * kMaxRank;
+    const int kb = k >> 4;
+    if ((k & 15) == ty) {
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+        if (ai == kb) {
+#pragma unroll
+          for (int bj = 0; bj < RB; ++bj) rowk[tx + 16 * bj] = a[ai][bj];
+        }
     }
-    int n = R - 1 - j;
-    int tri = n * (n + 1) / 2;
-    double inv = 1.0 / d;
-    for (int e = threadIdx.x; e < tri; e += blockDim.x) {
-      // e -> (i, k) with j < k <= i, row-major over the lower triangle
-      int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-      while ((i + 1) * (i + 2) / 2 <= e) ++i;
-      while (i * (i + 1) / 2 > e) --i;
-      int k = e - i * (i + 1) / 2;
-      int gi = j + 1 + i, gk = j + 1 + k;
-      A[gi * R + gk] -= A[gi * R + j] * A[gk * R + j] * inv;
+    if ((k & 15) == tx) {
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj)
+        if (bj == kb) {
+#pragma unroll
+          for (int ai = 0; ai < RB; ++ai) colk[ty + 16 * ai] = a[ai][bj];
+        }
     }
     __syncthreads();
+    const double p = rowk[k];
+    if (!(p > 0.0) || !isfinite(p)) return false;  // same p for every thread
+    const double inv = 1.0 / p;
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai) {
+      const int i = ty + 16 * ai;
+      const double cik = colk[i < R ? i : 0] * inv;
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) {
+        const int j = tx + 16 * bj;
+        const double rkj = rowk[j < R ? j : 0];
+        double v = a[ai][bj];
+        if (i == k)
+          v = (j == k) ? inv : v * inv;
+        else if (j == k)
+          v = -v * inv;
+        else
+          v = v - cik * rkj;
+        a[ai][bj] = v;
+      }
+    }
   }
-  __syncthreads();
-  bool ok = *bad == 0;
-  __syncthreads();
-  if (!ok) return false;
-  // scale columns: L_ij = a_ij / sqrt(a_jj), i >= j; zero the upper part
-  for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-    int i = e / R, j = e % R;
-    if (i < j) A[e] = 0.0;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
-    int i = e / R, j = e % R;
-    if (i > j) A[e] = A[e] / sqrt(A[j * R + j]);
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < R; j += blockDim.x) A[j * R + j] = sqrt(A[j * R + j]);
-  __syncthreads();
   return true;
 }
 
-__global__ void chol_kernel(AlsBuffers b, int ndim, int mode, int R, float ridge_eps, int last) {
-  extern __shared__ double sh[];
-  double* G = sh;            // R x R Hadamard; reused for L^{-1} once factored
-  double* L = sh + R * R;    // R x R Cholesky factor
-  double* W = G;
-  __shared__ int bad;
+template <int RB>
+__device__ void load_hadamard(const AlsBuffers& b, int ndim, int mode, int R, double ridge,
+                              double (&a)[RB][RB], bool write_h) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int RR = R * R;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int i = ty + 16 * ai, j = tx + 16 * bj;
+      double g = 0.0;
+      if (i < R && j < R) {
+        g = 1.0;  // compute_gram_hadamard starts from ones (helpers.rs:414)
+        for (int m = 0; m < ndim; ++m)
+          if (m != mode) g *= sym(b.grams + (int64_t)m * RR, R, i, j);
+        if (write_h) b.hadam[(int64_t)mode * RR + i * R + j] = g;
+        if (i == j) g += ridge;
+      } else if (i == j) {
+        g = 1.0;  // padding rows/cols: identity block, inverted harmlessly
+      }
+      a[ai][bj] = g;
+    }
+}
+
+// One CTA: G = Hadamard of the other Grams and G^-1 (ridge retry, as
+// solve_least_squares does, helpers.rs:477-490); zeroes this mode's Gram
+// accumulator (and <X,Xhat> for the last mode) for the solve that follows.
+template <int RB>
+__global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
+                                                   float ridge_eps, int last) {
+  __shared__ double prow[2 * kMaxRank], pcol[2 * kMaxRank];
   AlsState* st = b.state;
   if (st->done) return;
   const int RR = R * R;
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
-    double g = 1.0;  // compute_gram_hadamard starts from ones (helpers.rs:414)
-    for (int m = 0; m < ndim; ++m)
-      if (m != mode) g *= b.grams[(int64_t)m * RR + e];
-    G[e] = g;
-    b.hadam[(int64_t)mode * RR + e] = g;
-  }
-  __syncthreads();
+  double a[RB][RB];
+  load_hadamard<RB>(b, ndim, mode, R, 0.0, a, true);
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) L[e] = G[e];
-  __syncthreads();
-  bool ok = chol_inplace(L, R, &bad);
+  bool ok = gj_inverse_reg<RB>(a, prow, pcol, R);
   if (!ok) {
-    // helpers.rs:477-490: retry with eps * rank * 10 on the diagonal
-    for (int e = threadIdx.x; e < RR; e += blockDim.x)
-      L[e] = G[e] + ((e / R == e % R) ? (double)ridge_eps : 0.0);
     __syncthreads();
-    ok = chol_inplace(L, R, &bad);
+    load_hadamard<RB>(b, ndim, mode, R, (double)ridge_eps, a, false);
+    ok = gj_inverse_reg<RB>(a, prow, pcol, R);
     if (threadIdx.x == 0) st->ridge_used = 1;
     if (!ok) {
       if (threadIdx.x == 0) {
@@ -133,74 +203,58 @@ __global__ void chol_kernel(AlsBuffers b, int ndim, int mode, int R, float ridge
       return;
     }
   }
-  __syncthreads();  // G is dead from here on: W (= L^{-1}) takes its place
-  // W = L^{-1}: column c by forward substitution (thread per column).
-  for (int c = threadIdx.x; c < R; c += blockDim.x) {
-    for (int i = 0; i < R; ++i) {
-      if (i < c) {
-        W[i * R + c] = 0.0;
-        continue;
-      }
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int k = c; k < i; ++k) s -= L[i * R + k] * W[k * R + c];
-      W[i * R + c] = s / L[i * R + i];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int i = ty + 16 * ai, j = tx + 16 * bj;
+      if (i < R && j < R) b.ginv[i * R + j] = a[ai][bj];
     }
-  }
-  __syncthreads();
-  // G^{-1} = W^T W
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
-    int a = e / R, c = e % R;
-    int k0 = a > c ? a : c;
-    double s = 0.0;
-    for (int k = k0; k < R; ++k) s += W[k * R + a] * W[k * R + c];
-    b.ginv[e] = s;
-  }
-  // the Gram of U_mode is recomputed by the solve that follows
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) b.grams[(int64_t)mode * RR + e] = 0.0;
+  double* gm = b.grams + (int64_t)mode * RR;
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) gm[e] = 0.0;
   if (last && threadIdx.x == 0) st->inner = 0.0;
 }
 
-// rows_per_cta rows of U_mode. Shared: Ginv (R x R), M (rows x R), U (rows x R).
-__global__ void solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits,
-                             int64_t rows, int R, int rows_per_cta, float* __restrict__ U,
-                             int mode, int last) {
+// rows_per_cta rows of U_mode = (sum over splits of the partial MTTKRP) . G^-1.
+// Shared: G^-1 (R x R) and M (rows_per_cta x R), both FP64.
+__global__ void __launch_bounds__(256)
+solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
+             int rows_per_cta, float* __restrict__ U, int last) {
   extern __shared__ double sh[];
   AlsState* st = b.state;
   if (st->done) return;
   const int RR = R * R;
   double* Gi = sh;
   double* Ms = sh + RR;
-  double* Us = Ms + rows_per_cta * R;
-  int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
-  int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+  const int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
   for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = b.ginv[e];
   const int64_t pstride = rows * R;
   for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
+    // 8 independent loads in flight per step; fixed summation order
     const float* p = partials + r0 * R + e;
     double s = 0.0;
-    for (int q = 0; q < splits; ++q) s += (double)__ldg(p + (int64_t)q * pstride);
+    int q = 0;
+    for (; q + 8 <= splits; q += 8) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = __ldg(p + (int64_t)(q + u) * pstride);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += (double)v[u];
+    }
+    for (; q < splits; ++q) s += (double)__ldg(p + (int64_t)q * pstride);
     Ms[e] = s;
   }
   __syncthreads();
   double ip = 0.0;
   for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
-    int i = e / R, c = e % R;
+    const int i = e / R, c = e % R;
     double s = 0.0;
     for (int k = 0; k < R; ++k) s += Ms[i * R + k] * Gi[k * R + c];
-    float v = (float)s;
+    const float v = (float)s;
     U[(r0 + i) * R + c] = v;
-    Us[e] = (double)v;
     ip += Ms[e] * (double)v;
-  }
-  __syncthreads();
-  double* gram = b.grams + (int64_t)mode * RR;
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
-    int a = e / R, c = e % R;
-    if (c < a) continue;
-    double s = 0.0;
-    for (int i = 0; i < nr; ++i) s += Us[i * R + a] * Us[i * R + c];
-    atomicAdd(gram + a * R + c, s);
-    if (c != a) atomicAdd(gram + c * R + a, s);
   }
   if (last) {
     for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
@@ -213,9 +267,11 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
   if (st->done) return;
   const int RR = R * R;
   const int last = ndim - 1;
+  const double* H = b.hadam + (int64_t)last * RR;
+  const double* g = b.grams + (int64_t)last * RR;
   double s = 0.0;
-  for (int e = threadIdx.x; e < RR; e += blockDim.x)
-    s += b.hadam[(int64_t)last * RR + e] * b.grams[(int64_t)last * RR + e];
+#pragma unroll 8
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) s += H[e] * sym(g, R, e / R, e % R);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   __shared__ double ws[32];
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
@@ -224,17 +280,17 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
   double rn = 0.0;
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) rn += ws[w];
   // helpers.rs:513-530
-  double xn = st->xnorm_sq;
-  double err_sq = xn + rn - 2.0 * st->inner;
-  double err = sqrt(fmax(err_sq, 0.0));
+  const double xn = st->xnorm_sq;
+  const double err_sq = xn + rn - 2.0 * st->inner;
+  const double err = sqrt(fmax(err_sq, 0.0));
   double fit = 1.0 - err / sqrt(xn);
   fit = fmin(fmax(fit, 0.0), 1.0);
   // core.rs:173-198
-  int iter = st->iter;
+  const int iter = st->iter;
   st->fit = fit;
   b.history[iter] = fit;
   if (iter > 0 && fit < st->prev_fit) st->osc += 1;
-  double change = fabs(fit - st->prev_fit);
+  const double change = fabs(fit - st->prev_fit);
   st->final_change = change;
   st->iter = iter + 1;
   if (iter > 0 && change < tol) {
@@ -252,63 +308,74 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
 
 }  // namespace
 
-int launch_gram(tsr_ctx* ctx, const float* U, int64_t rows, int R, double* gram) {
-  TSR_CUDA(cudaMemsetAsync(gram, 0, sizeof(double) * R * R, ctx->stream));
-  int rpc = 32;
-  while (rpc > 1 && (size_t)rpc * R * 8 > 48 * 1024) rpc /= 2;
-  unsigned grid = (unsigned)ceil_div(rows, rpc);
-  gram_kernel<<<grid, 256, (size_t)rpc * R * 8, ctx->stream>>>(U, rows, R, rpc, gram);
-  ctx->launches++;
-  TSR_CUDA(cudaGetLastError());
-  return TSR_OK;
+void init_als_attributes() {
+  cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-int launch_norm_sq(tsr_ctx* ctx, const float* X, int64_t n, AlsState* st) {
-  int grid = ctx->sm_count * 4;
-  norm_sq_kernel<<<grid, 256, 0, ctx->stream>>>(X, n, st);
-  ctx->launches++;
-  TSR_CUDA(cudaGetLastError());
-  return TSR_OK;
-}
-
-int launch_chol(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int mode, int R, float ridge_eps,
-                bool last) {
-  size_t smem = (size_t)2 * R * R * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    TSR_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  2 * kMaxRank * kMaxRank * 8));
-    attr_set = true;
+int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int R,
+                double* gram, bool zero_first) {
+  if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large", R);
+  if (zero_first) TSR_CUDA(cudaMemsetAsync(gram, 0, sizeof(double) * R * R, s));
+  int64_t ctas = std::min<int64_t>(ceil_div(rows, 16), 2 * ctx->sm_count);
+  int64_t rpc = ceil_div(rows, ctas);
+  ctas = ceil_div(rows, rpc);
+  const unsigned g = (unsigned)ctas;
+  switch ((R + 15) / 16) {
+    case 1: gram_kernel<1><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    case 2: gram_kernel<2><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    case 3: gram_kernel<3><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    case 4: gram_kernel<4><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    case 5: gram_kernel<5><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    case 6: gram_kernel<6><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
+    default: gram_kernel<7><<<g, 256, 0, s>>>(U, rows, R, rpc, gram); break;
   }
-  if (smem > 227 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
-  chol_kernel<<<1, 256, smem, ctx->stream>>>(b, ndim, mode, R, ridge_eps, last ? 1 : 0);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
 }
 
-int launch_solve(tsr_ctx* ctx, const AlsBuffers& b, const float* partials, int splits,
-                 int64_t rows, int R, float* U, int mode, bool last) {
-  // Rows per CTA: enough CTAs to spread the partial-sum reads over the SMs.
-  int rpc = (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, ctx->sm_count)));
-  size_t smem = (size_t)(R * R + 2 * rpc * R) * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    TSR_CUDA(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  200 * 1024));
-    attr_set = true;
+int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, AlsState* st) {
+  const int grid = ctx->sm_count * 8;
+  norm_sq_kernel<<<grid, 256, 0, s>>>(X, n, st);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
+                float ridge_eps, bool last) {
+  if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
+  const int lst = last ? 1 : 0;
+  switch ((R + 15) / 16) {
+    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
   }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
+                 int splits, int64_t rows, int R, float* U, bool last) {
+  // enough CTAs to spread the split-K partial reads over the SMs
+  const int rpc =
+      (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, ctx->sm_count)));
+  const size_t smem = (size_t)(R * R + rpc * R) * sizeof(double);
   if (smem > 200 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
-  unsigned grid = (unsigned)ceil_div(rows, rpc);
-  solve_kernel<<<grid, 256, smem, ctx->stream>>>(b, partials, splits, rows, R, rpc, U, mode,
-                                                 last ? 1 : 0);
+  solve_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, s>>>(b, partials, splits, rows, R,
+                                                                rpc, U, last ? 1 : 0);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
 }
 
-int launch_fit(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int R, double tol) {
-  fit_kernel<<<1, 256, 0, ctx->stream>>>(b, ndim, R, tol);
+int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol) {
+  fit_kernel<<<1, 256, 0, s>>>(b, ndim, R, tol);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

@@ -30,19 +30,20 @@ struct AlsBuffers {
   double* history;  // [max_iters]
 };
 
-// gram[m] = U^T U (FP64), zeroing first. rows x R row-major fp32 input.
-int launch_gram(tsr_ctx* ctx, const float* U, int64_t rows, int R, double* gram);
-// ||X||^2 into state->xnorm_sq (zeroed first).
-int launch_norm_sq(tsr_ctx* ctx, const float* X, int64_t n, AlsState* state);
-// Hadamard of all Grams except `mode`, Cholesky (ridge fallback), inverse.
-// Also zeroes gram[mode] (about to be recomputed) and, when `last`, state->inner.
-int launch_chol(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int mode, int R, float ridge_eps,
-                bool last);
-// U_mode = (sum of split partials) . G^{-1}; accumulates gram[mode] and,
-// when `last`, <M, U> into state->inner.
-int launch_solve(tsr_ctx* ctx, const AlsBuffers& b, const float* partials, int splits,
-                 int64_t rows, int R, float* U, int mode, bool last);
+void init_als_attributes();
+// Upper triangle of U^T U (FP64) accumulated into gram; zero_first memsets it.
+int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int R,
+                double* gram, bool zero_first);
+// ||X||^2 into state->xnorm_sq (which must be zero).
+int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, AlsState* state);
+// Hadamard of all Grams except `mode`, its inverse (ridge retry), and the
+// zeroing of gram[mode] (and, when `last`, state->inner) before the solve.
+int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
+                float ridge_eps, bool last);
+// U_mode = (sum of split partials) . G^{-1}; `last` accumulates <M, U>.
+int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
+                 int splits, int64_t rows, int R, float* U, bool last);
 // fit, fit_history, oscillation and convergence rules of cp/core.rs:173-198.
-int launch_fit(tsr_ctx* ctx, const AlsBuffers& b, int ndim, int R, double tol);
+int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol);
 
 }  // namespace tsr

@@ -85,7 +85,14 @@ struct tsr_ctx {
   void* pinned = nullptr;  // pinned host staging (grow-only)
   size_t pinned_bytes = 0;
   unsigned* d_status = nullptr;  // device status word
-  int launches = 0;              // kernels launched by this context (counter)
+  int64_t launches = 0;          // kernels launched by this context (counter)
+  // second stream + events for the overlapped ALS sweep
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev[24] = {};
+  // cached instantiated sweep graph and the arguments it was captured with
+  cudaGraphExec_t sweep_exec = nullptr;
+  std::vector<uint8_t> sweep_key;
+  int64_t sweep_launches = 0;  // kernels per sweep graph launch
 };
 
 namespace tsr {
@@ -120,6 +127,10 @@ int launch_unfold_f32(tsr_ctx* ctx, const float* X, const int64_t* shape, const 
                       float* out);
 int launch_unfold_bf16x2(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
                          __nv_bfloat16* hi, __nv_bfloat16* lo);
+
+// Raise the dynamic shared-memory limits of every kernel once per process
+// (before any stream capture).
+void init_kernel_attributes();
 
 // Factor pointer table passed by value to kernels.
 struct FactorTable {

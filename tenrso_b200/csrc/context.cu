@@ -101,15 +101,24 @@ Unfolding make_unfolding(int ndim, const int64_t* shape, int mode) {
 
 // X viewed as [A][I][B] (A = prod of modes before `mode`, B = prod after);
 // X_(mode)[i][a*B + b] = X[a][i][b]. For B >= 32 rows of B elements are
-// contiguous on both sides: plain coalesced copy, one CTA row per (a, i).
+// contiguous on both sides: a coalesced copy (16-byte vectors when B % 4 == 0),
+// grid-stride over the (a, i) rows.
 template <class Store>
 __global__ void unfold_copy_kernel(const float* __restrict__ X, int64_t A, int64_t I, int64_t B,
                                    int64_t ld, Store store) {
-  int64_t row = blockIdx.x;  // (a, i) pair, a-major
-  int64_t a = row / I, i = row % I;
-  const float* src = X + (a * I + i) * B;
-  int64_t dst = i * ld + a * B;
-  for (int64_t b = threadIdx.x; b < B; b += blockDim.x) store(dst + b, __ldg(src + b));
+  const int64_t nrows = A * I;
+  const bool vec = (B % 4) == 0 && ((uintptr_t)X & 15) == 0;
+  for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int64_t a = row / I, i = row % I;
+    const float* src = X + row * B;
+    const int64_t dst = i * ld + a * B;
+    if (vec) {
+      const float4* s4 = reinterpret_cast<const float4*>(src);
+      for (int64_t q = threadIdx.x; q < B / 4; q += blockDim.x) store.put4(dst + 4 * q, __ldg(s4 + q));
+    } else {
+      for (int64_t b = threadIdx.x; b < B; b += blockDim.x) store(dst + b, __ldg(src + b));
+    }
+  }
 }
 
 // Small-B case: 32x32 tiles over (a, i) through shared memory so that both the
@@ -137,7 +146,10 @@ __global__ void unfold_transpose_kernel(const float* __restrict__ X, int64_t A, 
 struct StoreF32 {
   float* out;
   __device__ void operator()(int64_t k, float v) const { out[k] = v; }
+  __device__ void put4(int64_t k, float4 v) const { *reinterpret_cast<float4*>(out + k) = v; }
 };
+// x = hi + lo with hi = bf16(x), lo = bf16(x - hi): the operand split of the
+// BF16x3 MTTKRP.
 struct StoreBF16x2 {
   __nv_bfloat16* hi;
   __nv_bfloat16* lo;
@@ -145,6 +157,19 @@ struct StoreBF16x2 {
     __nv_bfloat16 h = __float2bfloat16_rn(v);
     hi[k] = h;
     lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+  __device__ void put4(int64_t k, float4 v) const {
+    __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y), h23 = __floats2bfloat162_rn(v.z, v.w);
+    float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+    __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - f01.x, v.y - f01.y);
+    __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
+    uint2 hv, lv;
+    hv.x = *reinterpret_cast<uint32_t*>(&h01);
+    hv.y = *reinterpret_cast<uint32_t*>(&h23);
+    lv.x = *reinterpret_cast<uint32_t*>(&l01);
+    lv.y = *reinterpret_cast<uint32_t*>(&l23);
+    *reinterpret_cast<uint2*>(hi + k) = hv;
+    *reinterpret_cast<uint2*>(lo + k) = lv;
   }
 };
 
@@ -156,8 +181,8 @@ static int launch_unfold(tsr_ctx* ctx, const float* X, const int64_t* shape, con
   for (int m = u.mode + 1; m < u.ndim; ++m) B *= shape[m];
   const int64_t I = u.rows;
   if (B >= 32) {
-    if (A * I > INT32_MAX) return fail(TSR_E_UNSUPPORTED, "unfold: too many rows");
-    unfold_copy_kernel<<<(unsigned)(A * I), 256, 0, ctx->stream>>>(X, A, I, B, u.ld, store);
+    const unsigned grid = (unsigned)std::min<int64_t>(A * I, (int64_t)ctx->sm_count * 16);
+    unfold_copy_kernel<<<grid, 256, 0, ctx->stream>>>(X, A, I, B, u.ld, store);
   } else {
     dim3 grid((unsigned)ceil_div(I, 32), (unsigned)ceil_div(A, 32));
     if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "unfold: grid too large");
@@ -241,13 +266,17 @@ int tsr_ctx_create(int device, void* stream, tsr_ctx** out) {
     }
     c->own_stream = true;
   }
-  cudaError_t e = cudaMalloc(&c->d_status, 256);
+  cudaError_t e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking);
+  for (int i = 0; e == cudaSuccess && i < 24; ++i)
+    e = cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_status, 256);
   if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, 256);
   if (e != cudaSuccess) {
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return fail(TSR_E_CUDA, "status alloc: %s", cudaGetErrorString(e));
   }
+  init_kernel_attributes();
   *out = c;
   return TSR_OK;
 }
@@ -260,6 +289,10 @@ int tsr_ctx_destroy(tsr_ctx* ctx) {
     if (b.ptr) cudaFree(b.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->sweep_exec) cudaGraphExecDestroy(ctx->sweep_exec);
+  for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TSR_OK;

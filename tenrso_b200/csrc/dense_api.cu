@@ -198,7 +198,53 @@ void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
 
 // ---------------------------------------------------------------------------
 // CP-ALS driver (cp/core.rs:91-214) on a device-resident tensor.
+//
+// One ALS sweep runs on two streams so that the FP64 work overlaps the
+// MTTKRPs: the main stream carries MTTKRP_n -> solve_n, the aux stream
+// gram_{n-1} -> inverse_n (concurrent with MTTKRP_n) and the fit. The sweep is
+// captured once into a CUDA graph and replayed max_iters times; every kernel
+// returns at entry once the device-side stop flag is set, which reproduces the
+// reference's early exits without host round trips.
 // ---------------------------------------------------------------------------
+struct SweepArgs {
+  const float* dX;
+  int ndim;
+  int64_t shape[kMaxModes];
+  int R;
+  int precision;
+  double tol;
+  float ridge;
+  FactorTable ft;
+  const void* op_ptrs[3 * kMaxModes];
+  float* partials;
+  AlsBuffers b;
+};
+
+static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<ModeOperand>& ops) {
+  cudaStream_t A = ctx->stream, B = ctx->aux;
+  TSR_CUDA(cudaEventRecord(ctx->ev[0], A));
+  TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[0], 0));
+  for (int n = 0; n < a.ndim; ++n) {
+    const bool last = n == a.ndim - 1;
+    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last));
+    TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
+    float* partials;
+    int splits;
+    TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
+    TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
+    TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
+                         const_cast<float*>(a.ft.ptr[n]), last));
+    TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
+    TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
+    TSR_TRY(launch_gram(ctx, B, a.ft.ptr[n], a.shape[n], a.R,
+                        a.b.grams + (size_t)n * a.R * a.R, false));
+  }
+  TSR_TRY(launch_fit(ctx, B, a.b, a.ndim, a.R, a.tol));
+  TSR_CUDA(cudaEventRecord(ctx->ev[23], B));
+  TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[23], 0));
+  return TSR_OK;
+}
+
 int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int64_t rank,
                   int max_iters, double tol, const float* d_init, int precision,
                   double time_limit_s, float* d_out, tsr_cp_info* info) {
@@ -219,76 +265,118 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
   const int R = (int)rank;
   const int64_t n = numel(ndim, shape);
 
+  SweepArgs a;
+  std::memset(&a, 0, sizeof(a));  // the bytes of `a` are the graph cache key
+  a.dX = dX;
+  a.ndim = ndim;
+  for (int m = 0; m < ndim; ++m) a.shape[m] = shape[m];
+  a.R = R;
+  a.precision = precision;
+  a.tol = tol;
+  a.ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
+
   // factors live in d_out for the whole run (updated in place)
   int64_t ftotal = 0;
-  FactorTable ft{};
   for (int m = 0; m < ndim; ++m) {
-    ft.ptr[m] = d_out + ftotal;
-    ft.rows[m] = shape[m];
+    a.ft.ptr[m] = d_out + ftotal;
+    a.ft.rows[m] = shape[m];
     ftotal += shape[m] * R;
   }
   if (d_init != d_out)
     TSR_CUDA(cudaMemcpyAsync(d_out, d_init, sizeof(float) * ftotal, cudaMemcpyDeviceToDevice,
                              ctx->stream));
 
-  // state + FP64 buffers
+  // every buffer is sized before any capture (no allocation inside a graph)
   const int hist_n = std::max(max_iters, 1);
-  size_t gbytes = sizeof(double) * (size_t)(2 * ndim + 1) * R * R;
-  size_t sbytes = 256 + sizeof(double) * hist_n;
+  const size_t gbytes = sizeof(double) * (size_t)(2 * ndim + 1) * R * R;
+  const size_t sbytes = 256 + sizeof(double) * hist_n;
   void *gp, *sp;
   TSR_TRY(slot_get(ctx, SLOT_GRAMS, gbytes, &gp));
   TSR_TRY(slot_get(ctx, SLOT_STATE, sbytes, &sp));
-  AlsBuffers b;
-  b.grams = (double*)gp;
-  b.hadam = b.grams + (size_t)ndim * R * R;
-  b.ginv = b.hadam + (size_t)ndim * R * R;
-  b.state = (AlsState*)sp;
-  b.history = (double*)((char*)sp + 256);
+  a.b.grams = (double*)gp;
+  a.b.hadam = a.b.grams + (size_t)ndim * R * R;
+  a.b.ginv = a.b.hadam + (size_t)ndim * R * R;
+  a.b.state = (AlsState*)sp;
+  a.b.history = (double*)((char*)sp + 256);
   TSR_CUDA(cudaMemsetAsync(sp, 0, sbytes, ctx->stream));
+  TSR_CUDA(cudaMemsetAsync(gp, 0, gbytes, ctx->stream));
 
   // per-mode unfoldings, resident for the whole run (the reference re-unfolds
   // in every mttkrp call, mttkrp.rs:126)
   std::vector<ModeOperand> ops(ndim);
-  if (max_iters > 0)
-    for (int m = 0; m < ndim; ++m)
+  size_t pmax = 0;
+  if (max_iters > 0) {
+    for (int m = 0; m < ndim; ++m) {
       TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
-  TSR_TRY(launch_norm_sq(ctx, dX, n, b.state));
+      const bool tc = precision == TSR_PREC_BF16X3;
+      SplitPlan p = tc ? plan_tc(ctx, ops[m].u.rows, ops[m].u.cols, R)
+                       : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
+      pmax = std::max(pmax, partial_floats(p, ops[m].u.rows, R));
+      a.op_ptrs[3 * m] = ops[m].f32;
+      a.op_ptrs[3 * m + 1] = ops[m].hi;
+      a.op_ptrs[3 * m + 2] = ops[m].lo;
+    }
+    void* pp;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
+    a.partials = (float*)pp;
+  }
+  TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, a.b.state));
   for (int m = 0; m < ndim; ++m)
-    TSR_TRY(launch_gram(ctx, ft.ptr[m], shape[m], R, b.grams + (size_t)m * R * R));
+    TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
+                        a.b.grams + (size_t)m * R * R, false));
 
-  const float ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
-  bool time_limited = time_limit_s >= 0.0;
+  const bool time_limited = time_limit_s >= 0.0;
   bool stopped_by_time = false;
-  for (int iter = 0; iter < max_iters; ++iter) {
-    if (time_limited) {
+  if (!time_limited && max_iters > 0) {
+    // capture (or reuse) the sweep graph and replay it max_iters times
+    std::vector<uint8_t> key((const uint8_t*)&a, (const uint8_t*)&a + sizeof(a));
+    if (!ctx->sweep_exec || key != ctx->sweep_key) {
+      if (ctx->sweep_exec) {
+        cudaGraphExecDestroy(ctx->sweep_exec);
+        ctx->sweep_exec = nullptr;
+      }
+      cudaGraph_t g;
+      const int64_t before = ctx->launches;
+      TSR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_sweep(ctx, a, ops);
+      cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+      if (rc != TSR_OK) return rc;
+      TSR_CUDA(ce);
+      ctx->sweep_launches = ctx->launches - before;
+      ctx->launches = before;
+      cudaError_t ie = cudaGraphInstantiate(&ctx->sweep_exec, g, 0);
+      cudaGraphDestroy(g);
+      TSR_CUDA(ie);
+      ctx->sweep_key = key;
+    }
+    for (int iter = 0; iter < max_iters; ++iter) {
+      TSR_CUDA(cudaGraphLaunch(ctx->sweep_exec, ctx->stream));
+      ctx->launches += ctx->sweep_launches;
+    }
+  } else {
+    for (int iter = 0; iter < max_iters; ++iter) {
       AlsState hs;
-      TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+      TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
       TSR_CUDA(cudaStreamSynchronize(ctx->stream));
       if (hs.done) break;
-      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+      // core.rs:151-156: checked at the start of every iteration
+      const double el =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
       if (el > time_limit_s) {
         stopped_by_time = true;
         break;
       }
+      TSR_TRY(enqueue_sweep(ctx, a, ops));
     }
-    for (int mode = 0; mode < ndim; ++mode) {
-      bool last = mode == ndim - 1;
-      float* partials;
-      int splits;
-      TSR_TRY(run_mttkrp_partials(ctx, ops[mode], ft, R, precision, &partials, &splits));
-      TSR_TRY(launch_chol(ctx, b, ndim, mode, R, ridge, last));
-      TSR_TRY(launch_solve(ctx, b, partials, splits, shape[mode], R, const_cast<float*>(ft.ptr[mode]), mode,
-                               last));
-    }
-    TSR_TRY(launch_fit(ctx, b, ndim, R, tol));
   }
   AlsState hs;
-  TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   TSR_CUDA(cudaStreamSynchronize(ctx->stream));
   if (hs.status & DS_NOT_SPD)
     return fail(TSR_E_NOT_SPD,
                 "Linear algebra error: Gram matrix is not positive definite (ridge %g also "
-                "failed)", (double)ridge);
+                "failed)",
+                (double)a.ridge);
   if (info) {
     info->fit = hs.fit;
     info->iters = hs.iter;
@@ -300,10 +388,19 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
     info->final_fit_change = hs.final_change;
     info->ridge_used = hs.ridge_used;
     if (info->fit_history && hs.iter > 0)
-      TSR_CUDA(cudaMemcpy(info->fit_history, b.history, sizeof(double) * hs.iter,
+      TSR_CUDA(cudaMemcpy(info->fit_history, a.b.history, sizeof(double) * hs.iter,
                           cudaMemcpyDeviceToHost));
   }
   return TSR_OK;
+}
+
+void init_kernel_attributes() {
+  static bool done = false;
+  if (done) return;
+  init_tc_attributes();
+  init_simt_attributes();
+  init_als_attributes();
+  done = true;
 }
 
 }  // namespace tsr
@@ -408,6 +505,49 @@ int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
     ft.rows[m] = shape[m];
   }
   return mttkrp_device(ctx, d_tensor, ndim, shape, ft, (int)rank, mode, precision, d_out);
+}
+
+int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
+                               const int64_t* shape, const float* const* d_factors, int64_t rank,
+                               int mode, int precision, int iters, int flush_l2,
+                               double* ms_per_launch, int64_t* splits_out) {
+  if (!shape || !d_factors || !d_tensor || !ms_per_launch || iters <= 0)
+    return fail(TSR_E_INVALID_ARG, "invalid argument");
+  std::vector<int64_t> cols(ndim, rank);
+  TSR_TRY(validate_mttkrp(ndim, shape, ndim, shape, cols.data(), mode));
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = shape[m];
+  }
+  ModeOperand op;
+  TSR_TRY(prepare_mode(ctx, d_tensor, ndim, shape, mode, precision, 0, &op));
+  void* flush = nullptr;
+  const size_t flush_bytes = std::max<size_t>(2 * ctx->l2_bytes, 256u << 20);
+  if (flush_l2) TSR_TRY(slot_get(ctx, SLOT_MISC3, flush_bytes, &flush));
+  cudaEvent_t a, b;
+  TSR_CUDA(cudaEventCreate(&a));
+  TSR_CUDA(cudaEventCreate(&b));
+  double total = 0.0;
+  int splits = 0;
+  for (int i = 0; i < iters; ++i) {
+    if (flush_l2) TSR_CUDA(cudaMemsetAsync(flush, i & 0xff, flush_bytes, ctx->stream));
+    float* partials;
+    TSR_CUDA(cudaEventRecord(a, ctx->stream));
+    TSR_TRY(run_mttkrp_partials(ctx, op, ft, (int)rank, precision, &partials, &splits));
+    TSR_CUDA(cudaEventRecord(b, ctx->stream));
+    TSR_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    TSR_CUDA(cudaEventElapsedTime(&ms, a, b));
+    total += ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms_per_launch = total / iters;
+  if (splits_out) *splits_out = splits;
+  return TSR_OK;
 }
 
 int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,

@@ -42,6 +42,42 @@ __device__ __forceinline__ void kr_row_offsets(const KRSpec& s, uint32_t j, uint
   }
 }
 
+// Mixed-radix position of an unfolding column: idx[p] is the row of factor
+// U_{o_p}. Decomposed with divisions once; afterwards advanced by carries,
+// which need a division only when a digit wraps.
+struct KRCounter {
+  uint32_t idx[kMaxModes];
+
+  __device__ __forceinline__ void init(const KRSpec& s, uint32_t j) {
+#pragma unroll
+    for (int p = kMaxModes - 1; p >= 0; --p) {
+      idx[p] = 0;
+      if (p < s.n_other) {
+        const uint32_t q = j / s.size[p];
+        idx[p] = j - q * s.size[p];
+        j = q;
+      }
+    }
+  }
+
+  __device__ __forceinline__ void advance(const KRSpec& s, uint32_t d) {
+#pragma unroll
+    for (int p = kMaxModes - 1; p >= 0; --p) {
+      if (p < s.n_other && d != 0) {
+        const uint32_t v = idx[p] + d;
+        if (v < s.size[p]) {
+          idx[p] = v;
+          d = 0;
+        } else {
+          const uint32_t q = v / s.size[p];
+          idx[p] = v - q * s.size[p];
+          d = q;
+        }
+      }
+    }
+  }
+};
+
 // KR[j, c] for one column c given precomputed row offsets.
 __device__ __forceinline__ float kr_value(const KRSpec& s, const uint32_t* off, int c) {
   float v = __ldg(s.f[0] + off[0] + c);

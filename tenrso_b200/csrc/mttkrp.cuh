@@ -9,6 +9,9 @@ struct SplitPlan {
   int64_t k_per_split = 0;
 };
 
+void init_tc_attributes();
+void init_simt_attributes();
+
 // FP32 SIMT kernel (mttkrp_simt.cu).
 SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
 int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,

@@ -67,21 +67,35 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
       As[buf][kq * 4 + 3][m] = areg[it].w;
     }
   };
-  // B-tile mapping: thread -> (kk = tid / 8, 8 consecutive columns).
-  auto gen_b = [&](int64_t k0) {
-    int kk = tid / 8, c0 = (tid % 8) * 8;
-    int64_t j = k0 + kk;
-    if (j < kend) {
-      uint32_t off[kMaxModes];
-      kr_row_offsets(kr, (uint32_t)j, off);
+  // B-tile mapping: thread -> (kk = tid / 8, 8 consecutive columns). The
+  // factor values of the next K-step are loaded before the FMA loop of the
+  // current one and multiplied after it, so the L2 latency overlaps the math.
+  float braw[2][8];
+  uint32_t boff[kMaxModes];
+  bool bvalid = false;
+  auto gen_b_load = [&](int64_t k0) {
+    const int kk = tid / 8, c0 = (tid % 8) * 8;
+    const int64_t j = k0 + kk;
+    bvalid = j < kend;
+    kr_row_offsets(kr, (uint32_t)(bvalid ? j : kbeg), boff);
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        int c = n0 + c0 + e;
-        breg[e] = (c < R) ? kr_value(kr, off, c) : 0.f;
-      }
-    } else {
+    for (int e = 0; e < 8; ++e) {
+      const int c = n0 + c0 + e;
+      const int cc = c < R ? c : 0;
+      braw[0][e] = __ldg(kr.f[0] + boff[0] + cc);
+      braw[1][e] = kr.n_other > 1 ? __ldg(kr.f[1] + boff[1] + cc) : 1.f;
+    }
+  };
+  auto gen_b_finish = [&]() {
+    const int c0 = (tid % 8) * 8;
 #pragma unroll
-      for (int e = 0; e < 8; ++e) breg[e] = 0.f;
+    for (int e = 0; e < 8; ++e) {
+      const int c = n0 + c0 + e;
+      float v = braw[0][e] * braw[1][e];
+#pragma unroll
+      for (int q = 2; q < kMaxModes; ++q)
+        if (q < kr.n_other) v *= __ldg(kr.f[q] + boff[q] + (c < R ? c : 0));
+      breg[e] = (bvalid && c < R) ? v : 0.f;
     }
   };
   auto store_b = [&](int buf) {
@@ -93,7 +107,8 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
 
   if (nsteps > 0) {
     load_a(kbeg);
-    gen_b(kbeg);
+    gen_b_load(kbeg);
+    gen_b_finish();
     store_a(0);
     store_b(0);
   }
@@ -103,7 +118,7 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
     const bool more = s + 1 < nsteps;
     if (more) {
       load_a(kbeg + (int64_t)(s + 1) * BK);
-      gen_b(kbeg + (int64_t)(s + 1) * BK);
+      gen_b_load(kbeg + (int64_t)(s + 1) * BK);
     }
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
@@ -118,6 +133,7 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
         for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
     if (more) {
+      gen_b_finish();
       store_a(buf ^ 1);
       store_b(buf ^ 1);
     }
@@ -169,10 +185,16 @@ int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, i
   return TSR_OK;
 }
 
+void init_simt_attributes() {
+  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(float) * 2 * BK * (BM + 4 + BN)));
+}
+
 SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
   SplitPlan p;
   int64_t mt = ceil_div(rows, BM), nt = ceil_div(R, BN);
-  int64_t want = std::max<int64_t>(1, (int64_t)ctx->sm_count * 3 / (mt * nt));
+  // one full wave at two resident CTAs per SM (no tail wave)
+  int64_t want = std::max<int64_t>(1, (int64_t)ctx->sm_count * 2 / (mt * nt));
   int64_t steps = ceil_div(K, BK);
   want = std::min<int64_t>(want, steps);
   p.k_per_split = round_up(ceil_div(K, want), BK);
@@ -186,12 +208,6 @@ int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const K
   dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, BM), (unsigned)ceil_div(kr.R, BN));
   if (grid.y > 65535 || grid.z > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
   const size_t smem = sizeof(float) * 2 * BK * (BM + 4 + BN);
-  static bool attr = false;
-  if (!attr) {
-    TSR_CUDA(cudaFuncSetAttribute(mttkrp_f32_splitk_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
   mttkrp_f32_splitk_kernel<<<grid, NT, smem, ctx->stream>>>(A, u.rows, u.cols, u.ld, kr,
                                                             plan.k_per_split, partials);
   ctx->launches++;

@@ -50,70 +50,122 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
-template <bool VEC4>
-__device__ __forceinline__ void kr_produce_stage(const TcParams& p, uint8_t* b_hi, uint8_t* b_lo,
-                                                 int64_t kbase, int64_t kend, int t) {
-  const int kq = t & 7;   // which 8-wide k chunk of the 64-wide stage
-  const int ng = t >> 3;  // 16 groups of 4 columns per 64-column pass
-  const KRSpec& kr = p.kr;
-  const int R = kr.R;
-  uint32_t off[8][kMaxModes];
-  bool valid[8];
+// Convert 8 consecutive-k values of one KR column into bf16 hi/lo and store
+// them as one 16-byte chunk of the swizzled K-major B operand (row n, chunk
+// kq ^ (n & 7)).
+__device__ __forceinline__ void store_kr_chunk(uint8_t* b_hi, uint8_t* b_lo, int n, int kq,
+                                               const float (&v)[8]) {
+  float h[8], l[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
-    int64_t j = kbase + kq * 8 + e;
-    valid[e] = j < kend;
-    if (valid[e]) kr_row_offsets(kr, (uint32_t)j, off[e]);
+    __nv_bfloat16 hb = __float2bfloat16_rn(v[e]);
+    h[e] = __bfloat162float(hb);
+    l[e] = v[e] - h[e];
   }
-  for (int nb = 0; nb < p.n_pad; nb += 64) {
-    const int n0 = nb + ng * 4;
-    if (n0 >= p.n_pad) break;
-    float v[8][4];
+  uint4 hv = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]),
+                        pack_bf16x2(h[4], h[5]), pack_bf16x2(h[6], h[7]));
+  uint4 lv = make_uint4(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]),
+                        pack_bf16x2(l[4], l[5]), pack_bf16x2(l[6], l[7]));
+  const uint32_t byte = (uint32_t)n * 128u + ((uint32_t)(kq ^ (n & 7)) << 4);
+  *reinterpret_cast<uint4*>(b_hi + byte) = hv;
+  *reinterpret_cast<uint4*>(b_lo + byte) = lv;
+}
+
+// Row positions of the 8 KR rows j0 .. j0+7 a producer thread covers.
+struct KRRows {
+  uint32_t idx[8][kMaxModes];
+  bool keep[8];
+};
+
+__device__ __forceinline__ void kr_rows(const KRSpec& kr, const KRCounter& c0, int64_t j0,
+                                        int64_t kend, KRRows& r) {
+  KRCounter c = c0;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      if (!valid[e] || n0 >= R) {
+  for (int e = 0; e < 8; ++e) {
+    if (e > 0) c.advance(kr, 1);
+    r.keep[e] = j0 + e < kend;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) v[e][c] = 0.f;
-        continue;
-      }
-      if (VEC4) {
-        float4 a = __ldg(reinterpret_cast<const float4*>(kr.f[0] + off[e][0] + n0));
-        v[e][0] = a.x; v[e][1] = a.y; v[e][2] = a.z; v[e][3] = a.w;
-#pragma unroll
-        for (int q = 1; q < kMaxModes; ++q) {
-          if (q < kr.n_other) {
-            float4 b = __ldg(reinterpret_cast<const float4*>(kr.f[q] + off[e][q] + n0));
-            v[e][0] *= b.x; v[e][1] *= b.y; v[e][2] *= b.z; v[e][3] *= b.w;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) v[e][c] = (n0 + c < R) ? kr_value(kr, off[e], n0 + c) : 0.f;
-      }
-    }
-    // swizzled K-major store: row n, 16-byte chunk kq ^ (n & 7)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int n = n0 + c;
-      float h[8], l[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        __nv_bfloat16 hb = __float2bfloat16_rn(v[e][c]);
-        h[e] = __bfloat162float(hb);
-        l[e] = v[e][c] - h[e];
-      }
-      uint4 hv = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]),
-                            pack_bf16x2(h[4], h[5]), pack_bf16x2(h[6], h[7]));
-      uint4 lv = make_uint4(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]),
-                            pack_bf16x2(l[4], l[5]), pack_bf16x2(l[6], l[7]));
-      const uint32_t byte = (uint32_t)n * 128u + ((uint32_t)(kq ^ (n & 7)) << 4);
-      *reinterpret_cast<uint4*>(b_hi + byte) = hv;
-      *reinterpret_cast<uint4*>(b_lo + byte) = lv;
-    }
+    for (int p = 0; p < kMaxModes; ++p) r.idx[e][p] = r.keep[e] ? c.idx[p] : 0u;
   }
 }
 
-template <bool VEC4>
+// Prefetchable part of a stage (fast path: at most two other modes, R % 4 == 0,
+// R <= 64): the factor rows for this thread's 8 KR rows and 4 columns, and a
+// bit mask of the rows that lie inside this CTA's K range.
+struct KRLoads {
+  float4 a[8], b[8];
+  uint32_t keep;
+};
+
+__device__ __forceinline__ void kr_issue(const KRSpec& kr, const KRCounter& c0, int64_t j0,
+                                         int64_t kend, int nc, KRLoads& L) {
+  KRCounter c = c0;
+  L.keep = 0;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    if (e > 0) c.advance(kr, 1);
+    const bool k = j0 + e < kend;
+    L.keep |= (k ? 1u : 0u) << e;
+    const uint32_t i0 = k ? c.idx[0] : 0u, i1 = k ? c.idx[1] : 0u;
+    L.a[e] = __ldg(reinterpret_cast<const float4*>(kr.f[0] + i0 * kr.R + nc));
+    L.b[e] = kr.n_other > 1
+                 ? __ldg(reinterpret_cast<const float4*>(kr.f[1] + i1 * kr.R + nc))
+                 : make_float4(1.f, 1.f, 1.f, 1.f);
+  }
+}
+
+__device__ __forceinline__ void kr_finish(const KRLoads& L, int n0, bool col_ok, int kq,
+                                          uint8_t* b_hi, uint8_t* b_lo) {
+  float v[4][8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const bool ok = ((L.keep >> e) & 1u) && col_ok;
+    v[0][e] = ok ? L.a[e].x * L.b[e].x : 0.f;
+    v[1][e] = ok ? L.a[e].y * L.b[e].y : 0.f;
+    v[2][e] = ok ? L.a[e].z * L.b[e].z : 0.f;
+    v[3][e] = ok ? L.a[e].w * L.b[e].w : 0.f;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) store_kr_chunk(b_hi, b_lo, n0 + c, kq, v[c]);
+}
+
+// General stage producer (any R, any number of modes): loads issued per
+// 64-column pass, then consumed.
+__device__ __forceinline__ void kr_produce_general(const TcParams& p, const KRRows& r,
+                                                   uint8_t* b_hi, uint8_t* b_lo, int t) {
+  const int kq = t & 7, ng = t >> 3;
+  const KRSpec& kr = p.kr;
+  const int R = kr.R;
+  for (int nb = 0; nb < p.n_pad; nb += 64) {
+    const int n0 = nb + ng * 4;
+    if (n0 >= p.n_pad) break;
+    float v[4][8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const bool ok = r.keep[e] && n0 + c < R;
+        const int col = ok ? n0 + c : 0;
+        v[c][e] = ok ? __ldg(kr.f[0] + r.idx[e][0] * R + col) : 0.f;
+      }
+#pragma unroll
+    for (int q = 1; q < kMaxModes; ++q) {
+      if (q < kr.n_other) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int col = n0 + c < R ? n0 + c : 0;
+            v[c][e] *= __ldg(kr.f[q] + r.idx[e][q] * R + col);
+          }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) store_kr_chunk(b_hi, b_lo, n0 + c, kq, v[c]);
+  }
+}
+
+template <bool VEC4, bool FAST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
                      const __grid_constant__ CUtensorMap map_lo, TcParams p) {
@@ -222,11 +274,28 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
       mma_commit(done);  // tracks every MMA issued above (also on abort)
     }
   } else {
-    // Khatri-Rao producers (warps 2..5, 128 threads)
+    // Khatri-Rao producers (warps 2..5, 128 threads). Thread t covers KR rows
+    // kbase + 8*(t & 7) .. +7 and columns 4*(t >> 3) .. +3 of each 64-column
+    // pass. Row positions advance by a mixed-radix counter (no division per
+    // row). On the fast path the factor loads of stage it+1 are issued before
+    // stage it is converted, so their L2 latency overlaps the work.
     const int t = threadIdx.x - 64;
-    for (int it = 0; it < nsteps; ++it) {
+    const int kq = t & 7;
+    const int n0 = (t >> 3) * 4;
+    KRCounter ctr;
+    ctr.init(p.kr, (uint32_t)(kbeg + kq * 8));
+    KRLoads loads[2];
+    constexpr bool fast = FAST;
+    const bool col_ok = n0 < p.kr.R;
+    const int nc = col_ok ? n0 : 0;
+    const bool active = n0 < p.n_pad;
+    auto stage = [&](int it, KRLoads& cur, KRLoads& nxt) -> bool {
       const int s = it % S;
       const uint32_t ph = (uint32_t)(it / S) & 1u;
+      if (fast && active && it + 1 < nsteps) {
+        ctr.advance(p.kr, TC_BK);
+        kr_issue(p.kr, ctr, kbeg + (int64_t)(it + 1) * TC_BK + kq * 8, kend, nc, nxt);
+      }
       int ok = 1;
       if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, abort_flag, WAIT_BUDGET) ? 1 : 0;
       ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -235,14 +304,28 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
           *abort_flag = 1;
           atomicOr(p.status, DS_TIMEOUT);
         }
-        break;
+        return false;
       }
       uint8_t* st = stage_ptr(s);
-      kr_produce_stage<VEC4>(p, st + 2 * A_TILE_BYTES, st + 2 * A_TILE_BYTES + b_bytes,
-                             kbeg + (int64_t)it * TC_BK, kend, t);
+      uint8_t* bh = st + 2 * A_TILE_BYTES;
+      uint8_t* bl = bh + b_bytes;
+      if (fast) {
+        if (active) kr_finish(cur, n0, col_ok, kq, bh, bl);
+      } else {
+        if (it > 0) ctr.advance(p.kr, TC_BK);
+        KRRows rows;
+        kr_rows(p.kr, ctr, kbeg + (int64_t)it * TC_BK + kq * 8, kend, rows);
+        if (!FAST) kr_produce_general(p, rows, bh, bl, t);
+      }
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&kr_full[s]);
+      return true;
+    };
+    if (fast && active && nsteps > 0) kr_issue(p.kr, ctr, kbeg + kq * 8, kend, nc, loads[0]);
+    for (int it = 0; it < nsteps; it += 2) {
+      if (!stage(it, loads[0], loads[1])) break;
+      if (it + 1 < nsteps && !stage(it + 1, loads[1], loads[0])) break;
     }
     // epilogue: TMEM accumulator -> split-K partial rows
     int ok = 1;
@@ -321,7 +404,16 @@ int stages_for(int n_pad) {
   return s > 4 ? 4 : s;
 }
 
+constexpr int kTcMaxSmem = 227 * 1024;
+
 }  // namespace
+
+void init_tc_attributes() {
+  cudaFuncSetAttribute(mttkrp_bf16x3_kernel<true, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, kTcMaxSmem);
+  cudaFuncSetAttribute(mttkrp_bf16x3_kernel<false, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, kTcMaxSmem);
+}
 
 bool tc_supported(const Unfolding& u, int R) {
   return R >= 1 && n_pad_of(R) <= 256 && u.cols < (int64_t)INT32_MAX && u.rows < INT32_MAX;
@@ -364,15 +456,12 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
   size_t smem = 1024 + (size_t)p.stages * stage + 8 * (3 * p.stages + 1) + 16;
   dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, TC_BM));
   if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
-  if (vec4) {
-    TSR_CUDA(cudaFuncSetAttribute(mttkrp_bf16x3_kernel<true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mttkrp_bf16x3_kernel<true><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
-  } else {
-    TSR_CUDA(cudaFuncSetAttribute(mttkrp_bf16x3_kernel<false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mttkrp_bf16x3_kernel<false><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
-  }
+  if (smem > kTcMaxSmem) return fail(TSR_E_UNSUPPORTED, "MTTKRP stage ring too large");
+  const bool fast = vec4 && p.n_pad <= 64 && kr.n_other <= 2;
+  if (fast)
+    mttkrp_bf16x3_kernel<true, true><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
+  else
+    mttkrp_bf16x3_kernel<false, false><<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, p);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

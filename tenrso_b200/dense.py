@@ -271,3 +271,19 @@ def cp_als_dev(d_tensor: int, shape, rank: int, max_iters: int, tol: float, d_in
                                          -1.0 if time_limit is None else float(time_limit),
                                          C.c_void_p(d_out), C.byref(info)))
     return float(info.fit), int(info.iters), _info_to(info, hist)
+
+
+def profile_mttkrp_dev(d_tensor: int, shape, d_factors: Sequence[int], rank: int, mode: int,
+                       precision="bf16x3", iters: int = 10, flush_l2: bool = True,
+                       ctx: Optional[Context] = None):
+    """Mean milliseconds of one MTTKRP kernel launch (operands prepared once),
+    and the split-K count used. Measurement aid for the roofline figure."""
+    shp = _i64(shape)
+    ptrs = (C.c_void_p * len(d_factors))(*d_factors)
+    ms = C.c_double(0)
+    splits = C.c_int64(0)
+    check(_lib.load().tsr_profile_mttkrp_dev_f32(_ctx_handle(ctx), C.c_void_p(d_tensor),
+                                                 len(shape), _ptr(shp), ptrs, rank, mode,
+                                                 _prec(precision), iters, int(flush_l2),
+                                                 C.byref(ms), C.byref(splits)))
+    return ms.value, splits.value
