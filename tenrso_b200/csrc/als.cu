@@ -96,82 +96,171 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, AlsState*
   }
 }
 
-// Gauss-Jordan inverse of the R x R Hadamard G without pivoting, register
-// blocked: thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns
-// tx + 16b (RB x RB doubles). Each pivot step publishes row k and column k
-// through double-buffered shared vectors (one barrier per step); all updates
-// are register FMAs. An SPD matrix has only positive pivots, so a pivot that
-// is not positive (or not finite) reports "not SPD" (uniformly across the CTA).
+// Block Gauss-Jordan inverse of the (padded) Hadamard G, no pivoting, 16 x 16
+// pivot blocks. Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and
+// columns tx + 16b (RB x RB doubles in registers). Block step K:
+//   P = G[K][K] is inverted by warp 0 (scalar Gauss-Jordan in shared memory,
+//     __syncwarp between its 16 pivots);
+//   G[K][j] <- P^-1 G[K][j],  G[i][K] <- -G[i][K] P^-1,
+//   G[i][j] <- G[i][j] - G[i][K] P^-1 G[K][j],  G[K][K] <- P^-1.
+// After the last block G holds G^-1. Every scalar pivot met on the way is a
+// pivot of G's LDL^T factorisation, so all are positive iff G is SPD; a pivot
+// that is not positive or not finite reports "not SPD" (uniform across the CTA).
 template <int RB>
-__device__ bool gj_inverse_reg(double (&a)[RB][RB], double* prow, double* pcol, int R) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  for (int k = 0; k < R; ++k) {
-    double* rowk = prow + (k & 1) * kMaxRank;
-    double* colk = pcol + (k & 1) * kMaxRank;
-    const int kb = k >> 4;
-    if ((k & 15) == ty) {
+struct GjShared {
+  double P[16][17];
+  double rowK[16][16 * RB];
+  double rowK2[16][16 * RB];
+  double colK[16 * RB][17];
+  int bad;
+};
+
+// 16 x 16 Gauss-Jordan inverse held by one warp: lane owns P[r][c] for
+// r = (lane >> 4) + 2q (q < 8), c = lane & 15. Pivot rows/columns move by
+// shuffles; returns false on a pivot that is not positive or not finite.
+__device__ __forceinline__ bool warp_gj16(double (&v)[8], int lane) {
+  const int c = lane & 15, r0 = lane >> 4;
+  bool ok = true;
 #pragma unroll
-      for (int ai = 0; ai < RB; ++ai)
-        if (ai == kb) {
+  for (int k = 0; k < 16; ++k) {
+    const int krow_lane = (k & 1) * 16;  // lanes holding row k
+    const double p = __shfl_sync(0xffffffffu, v[k >> 1], krow_lane + k);
+    const double pkc = __shfl_sync(0xffffffffu, v[k >> 1], krow_lane + c);
+    double prk[8];
 #pragma unroll
-          for (int bj = 0; bj < RB; ++bj) rowk[tx + 16 * bj] = a[ai][bj];
-        }
+    for (int q = 0; q < 8; ++q) prk[q] = __shfl_sync(0xffffffffu, v[q], r0 * 16 + k);
+    ok = ok && (p > 0.0) && isfinite(p);
+    const double inv = __drcp_rn(p);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int r = r0 + 2 * q;
+      if (r == k)
+        v[q] = (c == k) ? inv : v[q] * inv;
+      else if (c == k)
+        v[q] = -prk[q] * inv;
+      else
+        v[q] = v[q] - prk[q] * (pkc * inv);
     }
-    if ((k & 15) == tx) {
+  }
+  return ok;
+}
+
+template <int RB>
+__device__ bool gj_inverse_block(double (&a)[RB][RB], GjShared<RB>& sh) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) sh.bad = 0;
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj)
-        if (bj == kb) {
+  for (int K = 0; K < RB; ++K) {
+    // publish row block K, column block K and the pivot block
 #pragma unroll
-          for (int ai = 0; ai < RB; ++ai) colk[ty + 16 * ai] = a[ai][bj];
-        }
+    for (int bj = 0; bj < RB; ++bj) sh.rowK[ty][tx + 16 * bj] = a[K][bj];
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai) sh.colK[ty + 16 * ai][tx] = a[ai][K];
+    sh.P[ty][tx] = a[K][K];
+    __syncthreads();
+    if (warp == 0) {
+      double v[8];
+      const int c = lane & 15, r0 = lane >> 4;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = sh.P[r0 + 2 * q][c];
+      const bool ok = warp_gj16(v, lane);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sh.P[r0 + 2 * q][c] = v[q];
+      if (lane == 0 && !ok) sh.bad = 1;
     }
     __syncthreads();
-    const double p = rowk[k];
-    if (!(p > 0.0) || !isfinite(p)) return false;  // same p for every thread
-    const double inv = 1.0 / p;
+    if (sh.bad) return false;  // uniform: read after the barrier
+    // rowK2 = P^-1 . G[K][:] for the row-block-K rows this thread owns
+    {
+      double acc[RB];
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai) {
-      const int i = ty + 16 * ai;
-      const double cik = colk[i < R ? i : 0] * inv;
+      for (int bj = 0; bj < RB; ++bj) acc[bj] = 0.0;
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) {
-        const int j = tx + 16 * bj;
-        const double rkj = rowk[j < R ? j : 0];
-        double v = a[ai][bj];
-        if (i == k)
-          v = (j == k) ? inv : v * inv;
-        else if (j == k)
-          v = -v * inv;
-        else
-          v = v - cik * rkj;
-        a[ai][bj] = v;
+      for (int m = 0; m < 16; ++m) {
+        const double pm = sh.P[ty][m];
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) acc[bj] += pm * sh.rowK[m][tx + 16 * bj];
+      }
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) sh.rowK2[ty][tx + 16 * bj] = acc[bj];
+    }
+    __syncthreads();
+    // rank-16 update, register blocked: per m, RB + RB shared loads feed
+    // RB x RB FMAs
+    double colacc[RB];
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai) colacc[ai] = 0.0;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      double x[RB], y[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) x[ai] = sh.colK[ty + 16 * ai][m];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) y[bj] = sh.rowK2[m][tx + 16 * bj];
+      const double pmx = sh.P[m][tx];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) {
+        colacc[ai] += x[ai] * pmx;
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj)
+          if (ai != K && bj != K) a[ai][bj] -= x[ai] * y[bj];
       }
     }
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai) {
+      if (ai == K) {
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj)
+          a[ai][bj] = (bj == K) ? sh.P[ty][tx] : sh.rowK2[ty][tx + 16 * bj];
+      } else {
+        a[ai][K] = -colacc[ai];
+      }
+    }
+    __syncthreads();  // shared row/column blocks are rewritten by the next step
   }
   return true;
 }
 
+// G(i, j) = prod_{m != mode} Gram_m(i, j) for this thread's RB x RB block. All
+// loads are issued before any store (grams and hadam are distinct buffers).
 template <int RB>
-__device__ void load_hadamard(const AlsBuffers& b, int ndim, int mode, int R, double ridge,
-                              double (&a)[RB][RB], bool write_h) {
+__device__ void load_hadamard(const double* __restrict__ grams, double* __restrict__ hadam,
+                              int ndim, int mode, int R, double ridge, double (&a)[RB][RB],
+                              bool write_h) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int RR = R * R;
 #pragma unroll
   for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
+    for (int bj = 0; bj < RB; ++bj) a[ai][bj] = 1.0;  // helpers.rs:414 starts from ones
+  for (int m = 0; m < ndim; ++m) {
+    if (m == mode) continue;
+    const double* g = grams + (int64_t)m * RR;
+    double v[RB][RB];
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) {
+        const int i = ty + 16 * ai, j = tx + 16 * bj;
+        v[ai][bj] = (i < R && j < R) ? __ldg(g + (i <= j ? i * R + j : j * R + i)) : 1.0;
+      }
+#pragma unroll
+    for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= v[ai][bj];
+  }
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
     for (int bj = 0; bj < RB; ++bj) {
       const int i = ty + 16 * ai, j = tx + 16 * bj;
-      double g = 0.0;
       if (i < R && j < R) {
-        g = 1.0;  // compute_gram_hadamard starts from ones (helpers.rs:414)
-        for (int m = 0; m < ndim; ++m)
-          if (m != mode) g *= sym(b.grams + (int64_t)m * RR, R, i, j);
-        if (write_h) b.hadam[(int64_t)mode * RR + i * R + j] = g;
-        if (i == j) g += ridge;
-      } else if (i == j) {
-        g = 1.0;  // padding rows/cols: identity block, inverted harmlessly
+        if (write_h) hadam[(int64_t)mode * RR + i * R + j] = a[ai][bj];
+        if (i == j) a[ai][bj] += ridge;
+      } else {
+        a[ai][bj] = (i == j) ? 1.0 : 0.0;  // padding: identity block, inverted harmlessly
       }
-      a[ai][bj] = g;
     }
 }
 
@@ -181,19 +270,19 @@ __device__ void load_hadamard(const AlsBuffers& b, int ndim, int mode, int R, do
 template <int RB>
 __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
                                                    float ridge_eps, int last) {
-  __shared__ double prow[2 * kMaxRank], pcol[2 * kMaxRank];
+  __shared__ GjShared<RB> gsh;
   AlsState* st = b.state;
   if (st->done) return;
   const int RR = R * R;
   double a[RB][RB];
-  load_hadamard<RB>(b, ndim, mode, R, 0.0, a, true);
+  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
-  bool ok = gj_inverse_reg<RB>(a, prow, pcol, R);
+  bool ok = gj_inverse_block<RB>(a, gsh);
   if (!ok) {
     __syncthreads();
-    load_hadamard<RB>(b, ndim, mode, R, (double)ridge_eps, a, false);
-    ok = gj_inverse_reg<RB>(a, prow, pcol, R);
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
+    ok = gj_inverse_block<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
     if (!ok) {
       if (threadIdx.x == 0) {
@@ -229,29 +318,50 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
   double* Ms = sh + RR;
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
   const int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = b.ginv[e];
+#pragma unroll 8
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
   const int64_t pstride = rows * R;
-  for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
-    // 8 independent loads in flight per step; fixed summation order
+  // every thread sums a strided subset of the split partials of one element
+  // (16 loads in flight per batch), then the groups combine in shared memory
+  const int ne = nr * R;
+  const int full = rows_per_cta * R;  // the host sized `red` from this
+  const int groups = full >= (int)blockDim.x ? 1 : (int)blockDim.x / full;
+  double* red = Ms + rows_per_cta * R;  // [groups][ne]
+  for (int t = threadIdx.x; t < ne * groups; t += blockDim.x) {
+    const int e = t % ne, g = t / ne;
     const float* p = partials + r0 * R + e;
     double s = 0.0;
-    int q = 0;
-    for (; q + 8 <= splits; q += 8) {
-      float v[8];
+    int q = g;
+    for (; q + 15 * groups < splits; q += 16 * groups) {
+      float v[16];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) v[u] = __ldg(p + (int64_t)(q + u) * pstride);
+      for (int u = 0; u < 16; ++u) v[u] = __ldg(p + (int64_t)(q + u * groups) * pstride);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) s += (double)v[u];
+      for (int u = 0; u < 16; ++u) s += (double)v[u];
     }
-    for (; q < splits; ++q) s += (double)__ldg(p + (int64_t)q * pstride);
+    for (; q < splits; q += groups) s += (double)__ldg(p + (int64_t)q * pstride);
+    red[g * ne + e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    double s = 0.0;
+    for (int g = 0; g < groups; ++g) s += red[g * ne + e];
     Ms[e] = s;
   }
   __syncthreads();
   double ip = 0.0;
   for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
     const int i = e / R, c = e % R;
-    double s = 0.0;
-    for (int k = 0; k < R; ++k) s += Ms[i * R + k] * Gi[k * R + c];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four chains for ILP
+    int k = 0;
+    for (; k + 4 <= R; k += 4) {
+      s0 += Ms[i * R + k] * Gi[k * R + c];
+      s1 += Ms[i * R + k + 1] * Gi[(k + 1) * R + c];
+      s2 += Ms[i * R + k + 2] * Gi[(k + 2) * R + c];
+      s3 += Ms[i * R + k + 3] * Gi[(k + 3) * R + c];
+    }
+    for (; k < R; ++k) s0 += Ms[i * R + k] * Gi[k * R + c];
+    const double s = (s0 + s1) + (s2 + s3);
     const float v = (float)s;
     U[(r0 + i) * R + c] = v;
     ip += Ms[e] * (double)v;
@@ -364,8 +474,10 @@ int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float*
                  int splits, int64_t rows, int R, float* U, bool last) {
   // enough CTAs to spread the split-K partial reads over the SMs
   const int rpc =
-      (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, ctx->sm_count)));
-  const size_t smem = (size_t)(R * R + rpc * R) * sizeof(double);
+      (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 2 * ctx->sm_count)));
+  const int ne = rpc * R;
+  const int groups = ne >= 256 ? 1 : 256 / ne;
+  const size_t smem = (size_t)(R * R + rpc * R + (size_t)groups * ne) * sizeof(double);
   if (smem > 200 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   solve_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, s>>>(b, partials, splits, rows, R,
                                                                 rpc, U, last ? 1 : 0);

@@ -86,6 +86,9 @@ struct tsr_ctx {
   size_t pinned_bytes = 0;
   unsigned* d_status = nullptr;  // device status word
   int64_t launches = 0;          // kernels launched by this context (counter)
+  // SMs the MTTKRP grids leave free so that the side-stream FP64 kernels of
+  // the ALS sweep (Gram, inverse, fit) run concurrently instead of queueing
+  int reserve_sms = 8;
   // second stream + events for the overlapped ALS sweep
   cudaStream_t aux = nullptr;
   cudaEvent_t ev[24] = {};

@@ -43,14 +43,17 @@ __device__ __forceinline__ void kr_row_offsets(const KRSpec& s, uint32_t j, uint
 }
 
 // Mixed-radix position of an unfolding column: idx[p] is the row of factor
-// U_{o_p}. Decomposed with divisions once; afterwards advanced by carries,
-// which need a division only when a digit wraps.
+// U_{o_p} for the first NO other modes (NO >= the tensor's n_other).
+// Decomposed with divisions once; afterwards advanced by small steps whose
+// carries are resolved by subtraction (no division, no if-converted divide
+// sequences in the unrolled hot loop).
+template <int NO>
 struct KRCounter {
-  uint32_t idx[kMaxModes];
+  uint32_t idx[NO];
 
   __device__ __forceinline__ void init(const KRSpec& s, uint32_t j) {
 #pragma unroll
-    for (int p = kMaxModes - 1; p >= 0; --p) {
+    for (int p = NO - 1; p >= 0; --p) {
       idx[p] = 0;
       if (p < s.n_other) {
         const uint32_t q = j / s.size[p];
@@ -62,17 +65,16 @@ struct KRCounter {
 
   __device__ __forceinline__ void advance(const KRSpec& s, uint32_t d) {
 #pragma unroll
-    for (int p = kMaxModes - 1; p >= 0; --p) {
+    for (int p = NO - 1; p >= 0; --p) {
       if (p < s.n_other && d != 0) {
-        const uint32_t v = idx[p] + d;
-        if (v < s.size[p]) {
-          idx[p] = v;
-          d = 0;
-        } else {
-          const uint32_t q = v / s.size[p];
-          idx[p] = v - q * s.size[p];
-          d = q;
+        uint32_t v = idx[p] + d;
+        uint32_t carry = 0;
+        while (v >= s.size[p]) {
+          v -= s.size[p];
+          ++carry;
         }
+        idx[p] = v;
+        d = carry;
       }
     }
   }

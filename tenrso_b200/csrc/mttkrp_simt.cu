@@ -194,7 +194,8 @@ SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
   SplitPlan p;
   int64_t mt = ceil_div(rows, BM), nt = ceil_div(R, BN);
   // one full wave at two resident CTAs per SM (no tail wave)
-  int64_t want = std::max<int64_t>(1, (int64_t)ctx->sm_count * 2 / (mt * nt));
+  int64_t want =
+      std::max<int64_t>(1, (int64_t)(ctx->sm_count - ctx->reserve_sms) * 2 / (mt * nt));
   int64_t steps = ceil_div(K, BK);
   want = std::min<int64_t>(want, steps);
   p.k_per_split = round_up(ceil_div(K, want), BK);

@@ -39,7 +39,9 @@ struct TcParams {
   int64_t k_per_split;
   int n_pad;
   int stages;
-  int tmem_cols;
+  int tmem_cols;   // total TMEM columns allocated (n_acc * acc_cols)
+  int acc_cols;    // columns per accumulator (power of two >= n_pad, >= 32)
+  int n_acc;       // independent fp32 accumulators (even, 2..8)
   KRSpec kr;
   float* partials;
   unsigned* status;
@@ -77,9 +79,9 @@ struct KRRows {
   bool keep[8];
 };
 
-__device__ __forceinline__ void kr_rows(const KRSpec& kr, const KRCounter& c0, int64_t j0,
-                                        int64_t kend, KRRows& r) {
-  KRCounter c = c0;
+__device__ __forceinline__ void kr_rows(const KRSpec& kr, const KRCounter<kMaxModes>& c0,
+                                        int64_t j0, int64_t kend, KRRows& r) {
+  KRCounter<kMaxModes> c = c0;
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     if (e > 0) c.advance(kr, 1);
@@ -97,10 +99,23 @@ struct KRLoads {
   uint32_t keep;
 };
 
-__device__ __forceinline__ void kr_issue(const KRSpec& kr, const KRCounter& c0, int64_t j0,
+__device__ __forceinline__ void kr_issue(const KRSpec& kr, const KRCounter<2>& c0, int64_t j0,
                                          int64_t kend, int nc, KRLoads& L) {
-  KRCounter c = c0;
+  KRCounter<2> c = c0;
   L.keep = 0;
+  if (kr.n_other > 1 && c.idx[1] + 7 < kr.size[1] && j0 + 7 < kend) {
+    // common case: the 8 rows share the slower factor's row and step through
+    // consecutive rows of the faster one
+    const float4 a0 = __ldg(reinterpret_cast<const float4*>(kr.f[0] + c.idx[0] * kr.R + nc));
+    const float* fb = kr.f[1] + c.idx[1] * kr.R + nc;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      L.a[e] = a0;
+      L.b[e] = __ldg(reinterpret_cast<const float4*>(fb + e * kr.R));
+    }
+    L.keep = 0xffu;
+    return;
+  }
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     if (e > 0) c.advance(kr, 1);
@@ -265,9 +280,18 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
           const uint64_t dal = desc_sw128_kmajor(a_lo + koff);
           const uint64_t dbh = desc_sw128_kmajor(b_hi + koff);
           const uint64_t dbl = desc_sw128_kmajor(b_lo + koff);
-          mma_bf16(tmem, dah, dbh, idesc, (it > 0 || kk > 0) ? 1u : 0u);
-          mma_bf16(tmem, dah, dbl, idesc, 1u);
-          mma_bf16(tmem, dal, dbh, idesc, 1u);
+          // The tensor core's fp32 accumulation truncates, so a long chain
+          // of accumulations drifts low. k-slices rotate over n_acc/2
+          // accumulators for hi.hi and n_acc/2 more for the (2^-8 smaller)
+          // correction products; the epilogue adds them in FP64.
+          const int half = p.n_acc >> 1;
+          const int g = it * (TC_BK / 16) + kk;  // k-slice index in this split
+          const uint32_t acc_hh = tmem + (uint32_t)((g % half) * p.acc_cols);
+          const uint32_t acc_cr = tmem + (uint32_t)((half + g % half) * p.acc_cols);
+          const uint32_t first = g < half ? 0u : 1u;
+          mma_bf16(acc_hh, dah, dbh, idesc, first);
+          mma_bf16(acc_cr, dah, dbl, idesc, first);
+          mma_bf16(acc_cr, dal, dbh, idesc, 1u);
         }
         mma_commit(&empty[s]);
       }
@@ -282,7 +306,7 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
     const int t = threadIdx.x - 64;
     const int kq = t & 7;
     const int n0 = (t >> 3) * 4;
-    KRCounter ctr;
+    KRCounter<FAST ? 2 : kMaxModes> ctr;
     ctr.init(p.kr, (uint32_t)(kbeg + kq * 8));
     KRLoads loads[2];
     constexpr bool fast = FAST;
@@ -292,9 +316,11 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
     auto stage = [&](int it, KRLoads& cur, KRLoads& nxt) -> bool {
       const int s = it % S;
       const uint32_t ph = (uint32_t)(it / S) & 1u;
-      if (fast && active && it + 1 < nsteps) {
-        ctr.advance(p.kr, TC_BK);
-        kr_issue(p.kr, ctr, kbeg + (int64_t)(it + 1) * TC_BK + kq * 8, kend, nc, nxt);
+      if constexpr (FAST) {
+        if (active && it + 1 < nsteps) {
+          ctr.advance(p.kr, TC_BK);
+          kr_issue(p.kr, ctr, kbeg + (int64_t)(it + 1) * TC_BK + kq * 8, kend, nc, nxt);
+        }
       }
       int ok = 1;
       if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, abort_flag, WAIT_BUDGET) ? 1 : 0;
@@ -312,17 +338,21 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
       if (fast) {
         if (active) kr_finish(cur, n0, col_ok, kq, bh, bl);
       } else {
-        if (it > 0) ctr.advance(p.kr, TC_BK);
-        KRRows rows;
-        kr_rows(p.kr, ctr, kbeg + (int64_t)it * TC_BK + kq * 8, kend, rows);
-        if (!FAST) kr_produce_general(p, rows, bh, bl, t);
+        if constexpr (!FAST) {
+          if (it > 0) ctr.advance(p.kr, TC_BK);
+          KRRows rows;
+          kr_rows(p.kr, ctr, kbeg + (int64_t)it * TC_BK + kq * 8, kend, rows);
+          kr_produce_general(p, rows, bh, bl, t);
+        }
       }
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&kr_full[s]);
       return true;
     };
-    if (fast && active && nsteps > 0) kr_issue(p.kr, ctr, kbeg + kq * 8, kend, nc, loads[0]);
+    if constexpr (FAST) {
+      if (active && nsteps > 0) kr_issue(p.kr, ctr, kbeg + kq * 8, kend, nc, loads[0]);
+    }
     for (int it = 0; it < nsteps; it += 2) {
       if (!stage(it, loads[0], loads[1])) break;
       if (it + 1 < nsteps && !stage(it + 1, loads[1], loads[0])) break;
@@ -337,13 +367,30 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
     const int R = p.kr.R;
     float* out = p.partials + (int64_t)blockIdx.x * p.rows * R + row * R;
     if (ok && nsteps > 0) {
+      // accumulators that never received a k-slice (short splits) are skipped
+      const int used = min(p.n_acc >> 1, nsteps * (TC_BK / 16));
       for (int c0 = 0; c0 < p.n_pad; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        double sum[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sum[i] = 0.0;
+        // up to 8 accumulators: all loads in flight, one wait
+        uint32_t r[8][16];
+        const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+          if (a < p.n_acc && (a % (p.n_acc >> 1)) < used)  // warp-uniform
+            tmem_ld16_nowait(base + (uint32_t)(a * p.acc_cols), r[a]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+          if (a < p.n_acc && (a % (p.n_acc >> 1)) < used) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) sum[i] += (double)__uint_as_float(r[a][i]);
+          }
         if (row < p.rows) {
 #pragma unroll
           for (int i = 0; i < 16; ++i)
-            if (c0 + i < R) out[c0 + i] = v[i];
+            if (c0 + i < R) out[c0 + i] = (float)sum[i];
         }
       }
     } else if (row < p.rows) {
@@ -424,7 +471,7 @@ SplitPlan plan_tc(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
   SplitPlan p;
   int64_t mt = ceil_div(rows, TC_BM);
   int64_t steps = ceil_div(K, TC_BK);
-  int64_t want = std::max<int64_t>(1, ctx->sm_count / mt);
+  int64_t want = std::max<int64_t>(1, (ctx->sm_count - ctx->reserve_sms) / mt);
   want = std::min<int64_t>(want, steps);
   int64_t steps_per = ceil_div(steps, want);
   p.k_per_split = steps_per * TC_BK;
@@ -445,8 +492,11 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
   p.k_per_split = plan.k_per_split;
   p.n_pad = n_pad_of(kr.R);
   p.stages = stages_for(p.n_pad);
-  p.tmem_cols = 32;
-  while (p.tmem_cols < p.n_pad) p.tmem_cols *= 2;
+  p.acc_cols = 32;
+  while (p.acc_cols < p.n_pad) p.acc_cols *= 2;
+  p.n_acc = 512 / p.acc_cols;
+  if (p.n_acc > 8) p.n_acc = 8;
+  p.tmem_cols = p.n_acc * p.acc_cols;
   p.kr = kr;
   p.partials = partials;
   p.status = ctx->d_status;
