@@ -144,6 +144,52 @@ int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
                        int precision, double time_limit_s, float* d_out_factors,
                        tsr_cp_info* info);
 
+/* ---- sparse: crates/tenrso-sparse --------------------------------------
+ * COO entries are `indices` (nnz x ndim, row-major int64) and `values`
+ * (nnz float32). Validation follows CooTensor::new (coo.rs:101-149). */
+typedef struct tsr_sparse tsr_sparse;
+
+/* CooTensor::sort (coo.rs:239-257): stable lexicographic sort, in place. */
+int tsr_coo_sort_f32(tsr_ctx* ctx, int64_t* indices, float* values, int64_t nnz, int ndim,
+                     const int64_t* shape);
+/* CooTensor::deduplicate (coo.rs:320-347): sort, then sum equal coordinates
+ * left to right in fp32 (insertion order); rewrites the first *nnz_out entries. */
+int tsr_coo_deduplicate_f32(tsr_ctx* ctx, int64_t* indices, float* values, int64_t nnz, int ndim,
+                            const int64_t* shape, int64_t* nnz_out);
+/* CsfTensor::from_coo (csf.rs:137-264), bit-exact arrays: fptr is
+ * ndim x (nnz+1) and fids ndim x max(nnz,1) (row l = level l); lens[2l] and
+ * lens[2l+1] receive len(fptr[l]) and len(fids[l]); vals_out gets nnz values
+ * (none for ndim == 1, as the reference). Every fptr level holds nnz offsets. */
+int tsr_csf_from_coo_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
+                         int ndim, const int64_t* shape, const int64_t* mode_order,
+                         int n_mode_order, int64_t* fptr, int64_t* fids, float* vals_out,
+                         int64_t* lens);
+/* Device-resident sparse tensor: one CSF per root mode, mode_order = [n, the
+ * other modes in ascending size]. Duplicates are kept (as from_coo). */
+int tsr_sparse_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
+                          int ndim, const int64_t* shape, tsr_sparse** out);
+int tsr_sparse_destroy(tsr_sparse* sp);
+int tsr_sparse_info(const tsr_sparse* sp, int mode, int64_t* nnz, int64_t* n_roots,
+                    int64_t* n_fibers);
+/* Sparse MTTKRP (no tenrso implementation; csf.rs:42 names it): the dense
+ * mttkrp math (mttkrp.rs:851-875) over the nonzeros. out: shape[mode] x rank. */
+int tsr_mttkrp_csf_f32(tsr_ctx* ctx, const tsr_sparse* sp, const float* const* factors,
+                       int64_t rank, int mode, float* out);
+int tsr_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, const float* const* d_factors,
+                           int64_t rank, int mode, float* d_out);
+/* Kernel timing of the CSF MTTKRP (measurement aid, no tenrso counterpart). */
+int tsr_profile_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp,
+                                   const float* const* d_factors, int64_t rank, int mode,
+                                   int iters, int flush_l2, double* ms_per_launch);
+/* Sparse CP-ALS (tenrso has none): cp_als's loop (cp/core.rs:91-214) with the
+ * CSF MTTKRP; FP32 factors, FP64 Gram/solve/fit. */
+int tsr_cp_als_sparse_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
+                          double tol, const float* init_factors, uint64_t seed,
+                          double time_limit_s, float* out_factors, tsr_cp_info* info);
+int tsr_cp_als_sparse_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
+                              double tol, const float* d_init, double time_limit_s,
+                              float* d_out_factors, tsr_cp_info* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,4 +23,6 @@ from .dense import (  # noqa: F401
     profile_mttkrp_dev,
 )
 
+from .sparse import CooError, CooTensor, CsfError, CsfTensor, SparseTensor  # noqa: F401
+
 __version__ = "0.1.0"

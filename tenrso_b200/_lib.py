@@ -52,6 +52,20 @@ SIGNATURES = {
                                  C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
     "tsr_cp_als_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_int,
                                      C.c_double, P, C.POINTER(CpInfo)]),
+    "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
+    "tsr_coo_deduplicate_f32": (C.c_int, [P, P, P, I64, C.c_int, P, PI64]),
+    "tsr_csf_from_coo_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, P, P, P, P]),
+    "tsr_sparse_create_f32": (C.c_int, [P, P, P, I64, C.c_int, P, C.POINTER(P)]),
+    "tsr_sparse_destroy": (C.c_int, [P]),
+    "tsr_sparse_info": (C.c_int, [P, C.c_int, PI64, PI64, PI64]),
+    "tsr_mttkrp_csf_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
+    "tsr_mttkrp_csf_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
+    "tsr_profile_mttkrp_csf_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, C.c_int, C.c_int,
+                                                 C.POINTER(C.c_double)]),
+    "tsr_cp_als_sparse_f32": (C.c_int, [P, P, I64, C.c_int, C.c_double, P, C.c_uint64, C.c_double,
+                                        P, C.POINTER(CpInfo)]),
+    "tsr_cp_als_sparse_dev_f32": (C.c_int, [P, P, I64, C.c_int, C.c_double, P, C.c_double, P,
+                                            C.POINTER(CpInfo)]),
 }
 
 _lib = None

@@ -10,6 +10,7 @@
 #include <limits>
 
 #include "als.cuh"
+#include "csf.cuh"
 #include "mttkrp.cuh"
 
 namespace tsr {
@@ -218,6 +219,7 @@ struct SweepArgs {
   const void* op_ptrs[3 * kMaxModes];
   float* partials;
   AlsBuffers b;
+  const tsr_sparse* sp;  // sparse source (CSF MTTKRP) instead of the dense unfoldings
 };
 
 static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<ModeOperand>& ops) {
@@ -228,9 +230,12 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
     const bool last = n == a.ndim - 1;
     TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last));
     TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
-    float* partials;
-    int splits;
-    TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
+    float* partials = a.partials;
+    int splits = 1;
+    if (a.sp)
+      TSR_TRY(launch_mttkrp_csf(ctx, A, a.sp, a.ft, a.R, n, partials));
+    else
+      TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
     TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
     TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
                          const_cast<float*>(a.ft.ptr[n]), last));
@@ -245,9 +250,10 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
   return TSR_OK;
 }
 
-int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int64_t rank,
-                  int max_iters, double tol, const float* d_init, int precision,
-                  double time_limit_s, float* d_out, tsr_cp_info* info) {
+int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
+                  const int64_t* shape, int64_t rank, int max_iters, double tol,
+                  const float* d_init, int precision, double time_limit_s, float* d_out,
+                  tsr_cp_info* info) {
   auto t_start = std::chrono::steady_clock::now();
   // core.rs:115-127
   if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
@@ -274,6 +280,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
   a.precision = precision;
   a.tol = tol;
   a.ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
+  a.sp = sp;
 
   // factors live in d_out for the whole run (updated in place)
   int64_t ftotal = 0;
@@ -290,22 +297,27 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
   const int hist_n = std::max(max_iters, 1);
   const size_t gbytes = sizeof(double) * (size_t)(2 * ndim + 1) * R * R;
   const size_t sbytes = 256 + sizeof(double) * hist_n;
-  void *gp, *sp;
+  void *gp, *stp;
   TSR_TRY(slot_get(ctx, SLOT_GRAMS, gbytes, &gp));
-  TSR_TRY(slot_get(ctx, SLOT_STATE, sbytes, &sp));
+  TSR_TRY(slot_get(ctx, SLOT_STATE, sbytes, &stp));
   a.b.grams = (double*)gp;
   a.b.hadam = a.b.grams + (size_t)ndim * R * R;
   a.b.ginv = a.b.hadam + (size_t)ndim * R * R;
-  a.b.state = (AlsState*)sp;
-  a.b.history = (double*)((char*)sp + 256);
-  TSR_CUDA(cudaMemsetAsync(sp, 0, sbytes, ctx->stream));
+  a.b.state = (AlsState*)stp;
+  a.b.history = (double*)((char*)stp + 256);
+  TSR_CUDA(cudaMemsetAsync(stp, 0, sbytes, ctx->stream));
   TSR_CUDA(cudaMemsetAsync(gp, 0, gbytes, ctx->stream));
 
   // per-mode unfoldings, resident for the whole run (the reference re-unfolds
   // in every mttkrp call, mttkrp.rs:126)
   std::vector<ModeOperand> ops(ndim);
   size_t pmax = 0;
-  if (max_iters > 0) {
+  if (max_iters > 0 && sp) {
+    for (int m = 0; m < ndim; ++m) pmax = std::max(pmax, (size_t)shape[m] * R);
+    void* pp;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
+    a.partials = (float*)pp;
+  } else if (max_iters > 0) {
     for (int m = 0; m < ndim; ++m) {
       TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
       const bool tc = precision == TSR_PREC_BF16X3;
@@ -320,7 +332,11 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
     TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
     a.partials = (float*)pp;
   }
-  TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, a.b.state));
+  if (sp)  // sum of squared values, FP64, computed when the tensor was built
+    TSR_CUDA(cudaMemcpyAsync(&a.b.state->xnorm_sq, &sp->norm_sq, sizeof(double),
+                             cudaMemcpyHostToDevice, ctx->stream));
+  else
+    TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, a.b.state));
   for (int m = 0; m < ndim; ++m)
     TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
                         a.b.grams + (size_t)m * R * R, false));
@@ -557,8 +573,8 @@ int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
   if (!shape || !d_tensor || !d_init || !d_out_factors)
     return fail(TSR_E_INVALID_ARG, "null argument");
   TSR_TRY(check_ctx(ctx));
-  return cp_als_device(ctx, d_tensor, ndim, shape, rank, max_iters, tol, d_init, precision,
-                       time_limit_s, d_out_factors, info);
+  return cp_als_device(ctx, d_tensor, nullptr, ndim, shape, rank, max_iters, tol, d_init,
+                       precision, time_limit_s, d_out_factors, info);
 }
 
 int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
@@ -590,8 +606,51 @@ int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* s
   void* df;
   TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * ftotal, &df));
   TSR_CUDA(cudaMemcpyAsync(df, init, sizeof(float) * ftotal, cudaMemcpyHostToDevice, ctx->stream));
-  TSR_TRY(cp_als_device(ctx, dX, ndim, shape, rank, max_iters, tol, (const float*)df, precision,
-                        time_limit_s, (float*)df, info));
+  TSR_TRY(cp_als_device(ctx, dX, nullptr, ndim, shape, rank, max_iters, tol, (const float*)df,
+                        precision, time_limit_s, (float*)df, info));
+  TSR_CUDA(cudaMemcpyAsync(out_factors, df, sizeof(float) * ftotal, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int tsr_cp_als_sparse_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
+                              double tol, const float* d_init, double time_limit_s,
+                              float* d_out_factors, tsr_cp_info* info) {
+  if (!sp || !d_init || !d_out_factors) return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(check_ctx(ctx));
+  return cp_als_device(ctx, nullptr, sp, sp->ndim, sp->shape, rank, max_iters, tol, d_init,
+                       TSR_PREC_FP32, time_limit_s, d_out_factors, info);
+}
+
+int tsr_cp_als_sparse_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
+                          double tol, const float* init_factors, uint64_t seed,
+                          double time_limit_s, float* out_factors, tsr_cp_info* info) {
+  if (!sp || !out_factors) return fail(TSR_E_INVALID_ARG, "null argument");
+  if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  for (int d = 0; d < sp->ndim; ++d)
+    if (rank > sp->shape[d])
+      return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  if (!(tol >= 0.0 && tol < 1.0)) return fail(TSR_E_INVALID_TOL, "Invalid tolerance: %g", tol);
+  TSR_TRY(check_ctx(ctx));
+  int64_t ftotal = 0;
+  for (int m = 0; m < sp->ndim; ++m) ftotal += sp->shape[m] * rank;
+  std::vector<float> init_buf;
+  const float* init = init_factors;
+  if (!init) {
+    init_buf.resize(ftotal);
+    int64_t off = 0;
+    for (int m = 0; m < sp->ndim; ++m) {
+      seeded_uniform(seed, 200 + m, sp->shape[m] * rank, init_buf.data() + off);
+      off += sp->shape[m] * rank;
+    }
+    init = init_buf.data();
+  }
+  void* df;
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * ftotal, &df));
+  TSR_CUDA(cudaMemcpyAsync(df, init, sizeof(float) * ftotal, cudaMemcpyHostToDevice, ctx->stream));
+  TSR_TRY(cp_als_device(ctx, nullptr, sp, sp->ndim, sp->shape, rank, max_iters, tol,
+                        (const float*)df, TSR_PREC_FP32, time_limit_s, (float*)df, info));
   TSR_CUDA(cudaMemcpyAsync(out_factors, df, sizeof(float) * ftotal, cudaMemcpyDeviceToHost,
                            ctx->stream));
   TSR_CUDA(cudaStreamSynchronize(ctx->stream));
