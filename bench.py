@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sparse", action="store_true")
+    ap.add_argument("--sparse-nnz", type=int, default=50_000_000)
     return ap.parse_args()
 
 
@@ -148,6 +150,73 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+SP_SHAPE = (100000, 80000, 10000)
+SP_RANK = 32
+SP_ITERS = 20
+SP_SEED = 0xC3
+
+
+def run_sparse(tb, torch, ctx, stream, args, world, dist):
+    """CSF CP-ALS on the Zipf(1.2) tensor: device-drawn raw COO, merged on the
+    device (CooTensor::deduplicate semantics), one CSF per mode, then 20 ALS
+    iterations at rank 32. Also times the CSF MTTKRP kernel alone."""
+    from tenrso_b200 import synth
+    nnz = args.sparse_nnz
+    cap = 12 * nnz
+    d_idx = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_val = torch.empty(cap, dtype=torch.float32, device="cuda")
+    t0 = time.perf_counter()
+    n_raw = tb.synth_zipf_coo_dev(SP_SHAPE, nnz, SP_SEED, d_idx.data_ptr(), d_val.data_ptr(),
+                                  cap, ctx=ctx)
+    t1 = time.perf_counter()
+    n = tb.coo_deduplicate_dev(d_idx.data_ptr(), d_val.data_ptr(), n_raw, SP_SHAPE, ctx=ctx)
+    t2 = time.perf_counter()
+    sp = tb.SparseTensor(ctx=ctx, d_indices=d_idx.data_ptr(), d_values=d_val.data_ptr(), nnz=n,
+                         shape=SP_SHAPE)
+    t3 = time.perf_counter()
+    del d_idx, d_val
+    torch.cuda.empty_cache()
+    init = synth.init_factors(SP_SHAPE, SP_RANK, SP_SEED)
+    flat = np.concatenate([f.ravel() for f in init])
+    dinit = torch.from_numpy(flat).cuda()
+    dout = torch.empty_like(dinit)
+    sp.cp_als_dev(SP_RANK, SP_ITERS, 0.0, dinit.data_ptr(), dout.data_ptr())  # warm-up
+    steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fit, iters, _ = sp.cp_als_dev(SP_RANK, SP_ITERS, 0.0, dinit.data_ptr(), dout.data_ptr())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    d_factors = [dinit.data_ptr() + 4 * sum(SP_SHAPE[:m]) * SP_RANK for m in range(3)]
+    modes = []
+    for mode in range(3):
+        kms = sp.profile_mttkrp_dev(d_factors, SP_RANK, mode, iters=5, flush_l2=True)
+        inf = sp.info(mode)
+        others = sum(SP_SHAPE[m] for m in range(3) if m != mode)
+        b_min = (8 * n + 8 * inf["fibers"] + 8 * inf["roots"] + 4 * others * SP_RANK
+                 + 4 * SP_SHAPE[mode] * SP_RANK)
+        modes.append({"mode": mode, "kernel_ms": kms, "roots": inf["roots"],
+                      "fibers": inf["fibers"], "bytes_min": b_min,
+                      "achieved_gbs": b_min / (kms * 1e-3) / 1e9})
+    sp.close()
+    return {"workload": f"CSF CP-ALS {SP_SHAPE[0]}x{SP_SHAPE[1]}x{SP_SHAPE[2]}, Zipf(1.2) indices "
+                        f"over seeded permutations, rank {SP_RANK}, {SP_ITERS} iterations",
+            "nnz": n, "raw_entries": n_raw, "duplicates_merged": n_raw - n,
+            "iter_per_s": SP_ITERS * world / (ms / 1e3), "ms_per_run": ms, "fit": fit,
+            "iters": iters, "synth_s": t1 - t0, "dedup_s": t2 - t1, "csf_build_s": t3 - t2,
+            "mttkrp": modes,
+            "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / 6549.4}
+
+
 def run_ours(args):
     import torch
     import tenrso_b200 as tb
@@ -265,6 +334,8 @@ def run_ours(args):
            "d2h_bytes_per_step": int(flat_init.nbytes + 64),
            "api": "tsr_cp_als_f32 (host pointers)"}
 
+    sparse = None if args.no_sparse else run_sparse(tb, torch, ctx, stream, args, world, dist)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as orc
@@ -297,7 +368,7 @@ def run_ours(args):
             "fit_mixed": fit_mixed, "fit_fp32": fit_fp32,
             "fit_abs_diff": abs(fit_mixed - fit_fp32),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": int(launches),
+            "gpu_launches": int(launches), "sparse": sparse,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -168,6 +168,20 @@ int tsr_csf_from_coo_f32(tsr_ctx* ctx, const int64_t* indices, const float* valu
  * other modes in ascending size]. Duplicates are kept (as from_coo). */
 int tsr_sparse_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
                           int ndim, const int64_t* shape, tsr_sparse** out);
+/* Same from device COO arrays (indices validated on the device). */
+int tsr_sparse_create_dev_f32(tsr_ctx* ctx, const int64_t* d_indices, const float* d_values,
+                              int64_t nnz, int ndim, const int64_t* shape, tsr_sparse** out);
+/* CooTensor::deduplicate on device arrays (in place, first *nnz_out entries). */
+int tsr_coo_deduplicate_dev_f32(tsr_ctx* ctx, int64_t* d_indices, float* d_values, int64_t nnz,
+                                int ndim, const int64_t* shape, int64_t* nnz_out);
+/* Seeded synthetic input (no tenrso counterpart): `nnz` distinct coordinates
+ * of per-mode Zipf(s_exp) indices over seeded permutations, as a raw COO in
+ * draw order (duplicates included) written to d_indices/d_values (room for
+ * `capacity` entries); *n_raw_out receives the raw entry count. Identical to
+ * tenrso_b200.synth.zipf_coo. */
+int tsr_synth_zipf_coo_dev(tsr_ctx* ctx, int ndim, const int64_t* shape, int64_t nnz,
+                           uint64_t seed, double s_exp, int64_t capacity, int64_t* d_indices,
+                           float* d_values, int64_t* n_raw_out);
 int tsr_sparse_destroy(tsr_sparse* sp);
 int tsr_sparse_info(const tsr_sparse* sp, int mode, int64_t* nnz, int64_t* n_roots,
                     int64_t* n_fibers);

@@ -23,6 +23,14 @@ from .dense import (  # noqa: F401
     profile_mttkrp_dev,
 )
 
-from .sparse import CooError, CooTensor, CsfError, CsfTensor, SparseTensor  # noqa: F401
+from .sparse import (  # noqa: F401
+    CooError,
+    CooTensor,
+    CsfError,
+    CsfTensor,
+    SparseTensor,
+    coo_deduplicate_dev,
+    synth_zipf_coo_dev,
+)
 
 __version__ = "0.1.0"

@@ -57,6 +57,10 @@ SIGNATURES = {
     "tsr_csf_from_coo_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, P, P, P, P]),
     "tsr_sparse_create_f32": (C.c_int, [P, P, P, I64, C.c_int, P, C.POINTER(P)]),
     "tsr_sparse_destroy": (C.c_int, [P]),
+    "tsr_sparse_create_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P, C.POINTER(P)]),
+    "tsr_coo_deduplicate_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P, PI64]),
+    "tsr_synth_zipf_coo_dev": (C.c_int, [P, C.c_int, P, I64, C.c_uint64, C.c_double, I64, P, P,
+                                         PI64]),
     "tsr_sparse_info": (C.c_int, [P, C.c_int, PI64, PI64, PI64]),
     "tsr_mttkrp_csf_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_mttkrp_csf_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),

@@ -610,24 +610,19 @@ int upload_coo(tsr_ctx* ctx, const int64_t* idx, const float* vals, int64_t nnz,
   return TSR_OK;
 }
 
-// coo.rs:239-257 (sort) and :320-347 (deduplicate) on the device.
-int coo_sort_dedup(tsr_ctx* ctx, int64_t* idx, float* vals, int64_t nnz, int ndim,
-                   const int64_t* shape, bool dedup, int64_t* nnz_out) {
-  TSR_TRY(check_shape(ndim, shape));
-  TSR_TRY(check_host_bounds(idx, nnz, ndim, shape));
+// coo.rs:239-257 (sort) and :320-347 (deduplicate) on device arrays; the
+// result (sorted, optionally merged) overwrites the first *nnz_out entries.
+int coo_sort_dedup_dev(tsr_ctx* ctx, int64_t* d_idx, float* d_vals, int64_t nnz, int ndim,
+                       const int64_t* shape, bool dedup, int64_t* nnz_out) {
   if (nnz_out) *nnz_out = nnz;
   if (nnz <= 1) return TSR_OK;  // deduplicate returns early (coo.rs:321-323)
   if (nnz >= (int64_t)INT32_MAX) return fail(TSR_E_UNSUPPORTED, "more than 2^31 - 1 entries");
-  TSR_TRY(check_ctx(ctx));
   cudaStream_t s = ctx->stream;
-  int64_t* d_idx;
-  float* d_vals;
-  TSR_TRY(upload_coo(ctx, idx, vals, nnz, ndim, &d_idx, &d_vals));
   int mo[kMaxModes];
   for (int d = 0; d < ndim; ++d) mo[d] = d;
   KeySpec ks;
   TSR_TRY(make_keyspec(ndim, shape, mo, &ks));
-  Arena ar, keep;
+  Arena ar;
   uint64_t* keys;
   uint32_t* pos;
   int rc = sort_entries(ctx, s, ar, d_idx, nnz, ks, key_bits(ndim, shape), &keys, &pos);
@@ -637,21 +632,17 @@ int coo_sort_dedup(tsr_ctx* ctx, int64_t* idx, float* vals, int64_t nnz, int ndi
     if (dedup)
       rc = level_fibers(ctx, s, ar, ar, keys, nnz, 1, UINT64_MAX, &heads, nullptr, &count);
     float* vout = nullptr;
-    int64_t* iout = nullptr;
     if (rc == TSR_OK) rc = ar.get(&vout, count);
-    if (rc == TSR_OK) rc = ar.get(&iout, count * ndim);
     if (rc == TSR_OK) {
       if (dedup)
         segment_sum_kernel<<<grid_for(ctx, count), 256, 0, s>>>(heads, count, nnz, pos, d_vals,
                                                                 vout);
       else
         leaf_kernel<<<grid_for(ctx, nnz), 256, 0, s>>>(keys, pos, d_vals, nnz, 1, nullptr, vout);
-      decode_kernel<<<grid_for(ctx, count), 256, 0, s>>>(keys, heads, count, ks, iout);
+      decode_kernel<<<grid_for(ctx, count), 256, 0, s>>>(keys, heads, count, ks, d_idx);
       ctx->launches += 2;
-      cudaError_t e = cudaMemcpyAsync(idx, iout, sizeof(int64_t) * count * ndim,
-                                      cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(vals, vout, sizeof(float) * count, cudaMemcpyDeviceToHost, s);
+      cudaError_t e = cudaMemcpyAsync(d_vals, vout, sizeof(float) * count,
+                                      cudaMemcpyDeviceToDevice, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) rc = fail(TSR_E_CUDA, "%s", cudaGetErrorString(e));
       if (nnz_out) *nnz_out = count;
@@ -659,6 +650,27 @@ int coo_sort_dedup(tsr_ctx* ctx, int64_t* idx, float* vals, int64_t nnz, int ndi
   }
   ar.release();
   return rc;
+}
+
+int coo_sort_dedup(tsr_ctx* ctx, int64_t* idx, float* vals, int64_t nnz, int ndim,
+                   const int64_t* shape, bool dedup, int64_t* nnz_out) {
+  TSR_TRY(check_shape(ndim, shape));
+  TSR_TRY(check_host_bounds(idx, nnz, ndim, shape));
+  if (nnz_out) *nnz_out = nnz;
+  if (nnz <= 1) return TSR_OK;
+  TSR_TRY(check_ctx(ctx));
+  int64_t* d_idx;
+  float* d_vals;
+  TSR_TRY(upload_coo(ctx, idx, vals, nnz, ndim, &d_idx, &d_vals));
+  int64_t count = nnz;
+  TSR_TRY(coo_sort_dedup_dev(ctx, d_idx, d_vals, nnz, ndim, shape, dedup, &count));
+  TSR_CUDA(cudaMemcpyAsync(idx, d_idx, sizeof(int64_t) * count * ndim, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(vals, d_vals, sizeof(float) * count, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (nnz_out) *nnz_out = count;
+  return TSR_OK;
 }
 
 int copy_level_u32_to_i64(const uint32_t* d, int64_t n, int64_t* host) {
@@ -736,20 +748,8 @@ int tsr_csf_from_coo_f32(tsr_ctx* ctx, const int64_t* indices, const float* valu
   return rc;
 }
 
-int tsr_sparse_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
-                          int ndim, const int64_t* shape, tsr_sparse** out) {
-  if (!shape || !out || (nnz > 0 && (!indices || !values)))
-    return fail(TSR_E_INVALID_ARG, "null argument");
-  *out = nullptr;
-  TSR_TRY(check_shape(ndim, shape));
-  TSR_TRY(check_host_bounds(indices, nnz, ndim, shape));
-  if (nnz >= (int64_t)INT32_MAX) return fail(TSR_E_UNSUPPORTED, "more than 2^31 - 1 entries");
-  for (int d = 0; d < ndim; ++d)
-    if (shape[d] >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "mode size >= 2^32");
-  TSR_TRY(check_ctx(ctx));
-  int64_t* d_idx;
-  float* d_vals;
-  TSR_TRY(upload_coo(ctx, indices, values, nnz, ndim, &d_idx, &d_vals));
+static int sparse_create(tsr_ctx* ctx, const int64_t* d_idx, const float* d_vals, int64_t nnz,
+                         int ndim, const int64_t* shape, tsr_sparse** out) {
   tsr_sparse* sp = new tsr_sparse();
   sp->device = ctx->device;
   sp->ndim = ndim;
@@ -780,6 +780,45 @@ int tsr_sparse_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* val
   cudaFree(dsum);
   *out = sp;
   return TSR_OK;
+}
+
+int tsr_sparse_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
+                          int ndim, const int64_t* shape, tsr_sparse** out) {
+  if (!shape || !out || (nnz > 0 && (!indices || !values)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  TSR_TRY(check_shape(ndim, shape));
+  TSR_TRY(check_host_bounds(indices, nnz, ndim, shape));
+  if (nnz >= (int64_t)INT32_MAX) return fail(TSR_E_UNSUPPORTED, "more than 2^31 - 1 entries");
+  for (int d = 0; d < ndim; ++d)
+    if (shape[d] >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "mode size >= 2^32");
+  TSR_TRY(check_ctx(ctx));
+  int64_t* d_idx;
+  float* d_vals;
+  TSR_TRY(upload_coo(ctx, indices, values, nnz, ndim, &d_idx, &d_vals));
+  return sparse_create(ctx, d_idx, d_vals, nnz, ndim, shape, out);
+}
+
+int tsr_sparse_create_dev_f32(tsr_ctx* ctx, const int64_t* d_indices, const float* d_values,
+                              int64_t nnz, int ndim, const int64_t* shape, tsr_sparse** out) {
+  if (!shape || !out || (nnz > 0 && (!d_indices || !d_values)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  TSR_TRY(check_shape(ndim, shape));
+  if (nnz >= (int64_t)INT32_MAX) return fail(TSR_E_UNSUPPORTED, "more than 2^31 - 1 entries");
+  for (int d = 0; d < ndim; ++d)
+    if (shape[d] >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "mode size >= 2^32");
+  TSR_TRY(check_ctx(ctx));
+  return sparse_create(ctx, d_indices, d_values, nnz, ndim, shape, out);
+}
+
+int tsr_coo_deduplicate_dev_f32(tsr_ctx* ctx, int64_t* d_indices, float* d_values, int64_t nnz,
+                                int ndim, const int64_t* shape, int64_t* nnz_out) {
+  if (!shape || !nnz_out || (nnz > 0 && (!d_indices || !d_values)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(check_shape(ndim, shape));
+  TSR_TRY(check_ctx(ctx));
+  return coo_sort_dedup_dev(ctx, d_indices, d_values, nnz, ndim, shape, true, nnz_out);
 }
 
 int tsr_sparse_destroy(tsr_sparse* sp) {

@@ -191,20 +191,49 @@ class CsfTensor:
         return CooTensor(idx, self._vals, self._shape)
 
 
+def synth_zipf_coo_dev(shape, nnz: int, seed: int, d_indices: int, d_values: int,
+                       capacity: int, s: float = 1.2, ctx=None) -> int:
+    """Device version of synth.zipf_coo: writes the raw COO (duplicates
+    included) to device buffers and returns its entry count."""
+    n = C.c_int64(0)
+    check(_lib.load().tsr_synth_zipf_coo_dev(_ctx_handle(ctx), len(shape), _ptr(_i64(shape)),
+                                             nnz, seed, float(s), capacity,
+                                             C.c_void_p(d_indices), C.c_void_p(d_values),
+                                             C.byref(n)))
+    return n.value
+
+
+def coo_deduplicate_dev(d_indices: int, d_values: int, nnz: int, shape, ctx=None) -> int:
+    """CooTensor::deduplicate on device arrays; returns the merged count."""
+    n = C.c_int64(0)
+    check(_lib.load().tsr_coo_deduplicate_dev_f32(_ctx_handle(ctx), C.c_void_p(d_indices),
+                                                  C.c_void_p(d_values), nnz, len(shape),
+                                                  _ptr(_i64(shape)), C.byref(n)))
+    return n.value
+
+
 class SparseTensor:
     """Device-resident sparse tensor for MTTKRP / CP-ALS (one CSF per mode)."""
 
-    def __init__(self, coo: CooTensor, ctx=None):
+    def __init__(self, coo: Optional[CooTensor] = None, ctx=None, *, d_indices: int = 0,
+                 d_values: int = 0, nnz: int = 0, shape=None):
         from .dense import default_context
         self._ctx = ctx or default_context()
         self._lib = _lib.load()
         h = C.c_void_p()
-        check(self._lib.tsr_sparse_create_f32(self._ctx.handle, _ptr(coo.indices()),
-                                              _ptr(coo.values()), coo.nnz(), coo.rank(),
-                                              _ptr(_i64(coo.shape())), C.byref(h)))
+        if coo is not None:
+            check(self._lib.tsr_sparse_create_f32(self._ctx.handle, _ptr(coo.indices()),
+                                                  _ptr(coo.values()), coo.nnz(), coo.rank(),
+                                                  _ptr(_i64(coo.shape())), C.byref(h)))
+            self.shape = coo.shape()
+            self.nnz = coo.nnz()
+        else:
+            check(self._lib.tsr_sparse_create_dev_f32(self._ctx.handle, C.c_void_p(d_indices),
+                                                      C.c_void_p(d_values), nnz, len(shape),
+                                                      _ptr(_i64(shape)), C.byref(h)))
+            self.shape = list(shape)
+            self.nnz = nnz
         self.handle = h
-        self.shape = coo.shape()
-        self.nnz = coo.nnz()
 
     def info(self, mode: int):
         nnz, roots, fibers = C.c_int64(), C.c_int64(), C.c_int64()

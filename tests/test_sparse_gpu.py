@@ -153,3 +153,24 @@ def test_sparse_cp_als_vs_dense_oracle(orc):
     assert res.iters == 12
     assert abs(res.fit - info["fit"]) <= 1e-4, (res.fit, info["fit"])
     sp.close()
+
+
+def test_device_zipf_generator_matches_numpy():
+    import torch
+    shape = (1000, 800, 100)
+    idx, vals, dups = synth.zipf_coo(shape, 20000, seed=0xC3)
+    cap = 4 * idx.shape[0]
+    d_idx = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_val = torch.empty(cap, dtype=torch.float32, device="cuda")
+    n = tb.synth_zipf_coo_dev(shape, 20000, 0xC3, d_idx.data_ptr(), d_val.data_ptr(), cap)
+    torch.cuda.synchronize()
+    assert n == idx.shape[0]
+    assert np.array_equal(d_idx[:n * 3].cpu().numpy().reshape(n, 3), idx)
+    assert np.array_equal(d_val[:n].cpu().numpy(), vals)
+    m = tb.coo_deduplicate_dev(d_idx.data_ptr(), d_val.data_ptr(), n, shape)
+    torch.cuda.synchronize()
+    assert m == 20000
+    coo = tb.CooTensor(idx, vals, shape)
+    coo.deduplicate()
+    assert np.array_equal(d_idx[:m * 3].cpu().numpy().reshape(m, 3), coo.indices())
+    assert np.array_equal(d_val[:m].cpu().numpy(), coo.values())
