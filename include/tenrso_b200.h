@@ -70,7 +70,8 @@ typedef struct tsr_cp_info {
   int32_t oscillation_count;
   double final_fit_change;
   double* fit_history;
-  int32_t ridge_used; /* the eps*rank*10 ridge of cp/helpers.rs:477-490 engaged */
+  int32_t ridge_used; /* 1: the eps*rank*10 ridge of cp/helpers.rs:477-490 engaged;
+                         2: that ridge scaled by the Gram's mean diagonal was needed */
   int32_t reserved;
 } tsr_cp_info;
 

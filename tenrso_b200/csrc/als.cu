@@ -112,6 +112,7 @@ struct GjShared {
   double rowK[16][16 * RB];
   double rowK2[16][16 * RB];
   double colK[16 * RB][17];
+  double scale;
   int bad;
 };
 
@@ -284,13 +285,33 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
     ok = gj_inverse_block<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
-    if (!ok) {
-      if (threadIdx.x == 0) {
-        st->status |= DS_NOT_SPD;
-        st->done = 1;
-      }
-      return;
+  }
+  if (!ok) {
+    // lstsq (the reference's solver) returns a least-squares solution for a
+    // numerically singular Gram; the Cholesky-type stand-in needs a ridge on
+    // the scale of G for that: eps * rank * 10 times the mean diagonal.
+    __syncthreads();
+    if (threadIdx.x == 0) gsh.scale = 0.0;
+    __syncthreads();
+    const double* H = b.hadam + (int64_t)mode * RR;
+    if (threadIdx.x < 32) {
+      double d = 0.0;
+      for (int i = threadIdx.x; i < R; i += 32) d += fabs(H[i * R + i]);
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+      if (threadIdx.x == 0) gsh.scale = d / R;
     }
+    __syncthreads();
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps * fmax(gsh.scale, 1.0),
+                      a, false);
+    ok = gj_inverse_block<RB>(a, gsh);
+    if (threadIdx.x == 0) st->ridge_used = 2;
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      st->status |= DS_NOT_SPD;
+      st->done = 1;
+    }
+    return;
   }
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll

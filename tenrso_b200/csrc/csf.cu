@@ -403,11 +403,13 @@ constexpr int CSF_THREADS = 256;
 constexpr int CSF_WMAX = 64;  // privatised root rows per CTA window
 
 template <int G>
-__global__ void __launch_bounds__(CSF_THREADS)
+__global__ void __launch_bounds__(CSF_THREADS, 2)
 csf3_mttkrp_kernel(Csf3Args a) {
   extern __shared__ float4 win[];  // [CSF_WMAX][G]
   constexpr int GPC = CSF_THREADS / G;
+  constexpr int NB = 8;  // entries whose factor rows are in flight together
   const int grp = threadIdx.x / G, sub = threadIdx.x % G;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int64_t blk = blockIdx.x; blk * GPC < a.n_chunks; blk += gridDim.x) {
     const int64_t c0 = blk * GPC;
     const int64_t c1 = min(c0 + (int64_t)GPC, a.n_chunks);
@@ -415,8 +417,7 @@ csf3_mttkrp_kernel(Csf3Args a) {
     const int64_t whi = c1 < a.n_chunks ? (int64_t)a.chunk_root[c1] : a.n_roots - 1;
     const bool priv = whi - wlo + 1 <= CSF_WMAX;
     if (priv) {
-      for (int i = threadIdx.x; i < (whi - wlo + 1) * G; i += CSF_THREADS)
-        win[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = threadIdx.x; i < (whi - wlo + 1) * G; i += CSF_THREADS) win[i] = zero4;
       __syncthreads();
     }
     const int64_t c = c0 + grp;
@@ -426,42 +427,73 @@ csf3_mttkrp_kernel(Csf3Args a) {
       int64_t s = a.chunk_root[c];
       int64_t f = a.chunk_fiber[c];
       int64_t root_end = a.root_ptr[s + 1];
-      int64_t fib_end = a.fib_ptr[f + 1];
-      float4 t = make_float4(0.f, 0.f, 0.f, 0.f), acc = t;
-      for (; k < kend; ++k) {
-        const uint32_t b = __ldg(a.leaf_ids + k);
-        const float v = __ldg(a.vals + k);
-        const float4 u = __ldg(reinterpret_cast<const float4*>(a.Ub + (size_t)b * a.R) + sub);
-        t.x = fmaf(v, u.x, t.x);
-        t.y = fmaf(v, u.y, t.y);
-        t.z = fmaf(v, u.z, t.z);
-        t.w = fmaf(v, u.w, t.w);
-        const bool fiber_done = k + 1 == fib_end;
-        if (fiber_done || k + 1 == kend) {
-          const uint32_t ai = __ldg(a.fib_ids + f);
-          const float4 w = __ldg(reinterpret_cast<const float4*>(a.Ua + (size_t)ai * a.R) + sub);
-          acc.x = fmaf(w.x, t.x, acc.x);
-          acc.y = fmaf(w.y, t.y, acc.y);
-          acc.z = fmaf(w.z, t.z, acc.z);
-          acc.w = fmaf(w.w, t.w, acc.w);
-          t = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (fiber_done && ++f < a.n_fibers) fib_end = __ldg(a.fib_ptr + f + 1);
-          const bool root_done = k + 1 == root_end;
-          if (root_done || k + 1 == kend) {
-            if (priv) {
-              float* r = reinterpret_cast<float*>(win + (s - wlo) * G + sub);
-              atomicAdd(r + 0, acc.x);
-              atomicAdd(r + 1, acc.y);
-              atomicAdd(r + 2, acc.z);
-              atomicAdd(r + 3, acc.w);
-            } else {
-              const uint32_t ri = __ldg(a.root_ids + s);
-              atomicAdd(reinterpret_cast<float4*>(a.M + (size_t)ri * a.R) + sub, acc);
+      // current fiber f and, one ahead, fiber f+1 (its end and factor row)
+      int64_t fib_end = __ldg(a.fib_ptr + f + 1);
+      float4 ua = __ldg(reinterpret_cast<const float4*>(a.Ua + (size_t)__ldg(a.fib_ids + f) * a.R) + sub);
+      int64_t nf_end = fib_end;
+      float4 n_ua = zero4;
+      if (f + 1 < a.n_fibers) {
+        nf_end = __ldg(a.fib_ptr + f + 2);
+        n_ua = __ldg(reinterpret_cast<const float4*>(a.Ua + (size_t)__ldg(a.fib_ids + f + 1) * a.R) + sub);
+      }
+      float4 t = zero4, acc = zero4;
+      while (k < kend) {
+        const int nb = (int)min((int64_t)NB, kend - k);
+        uint32_t b[NB];
+        float v[NB];
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          b[i] = i < nb ? __ldg(a.leaf_ids + k + i) : 0u;
+          v[i] = i < nb ? __ldg(a.vals + k + i) : 0.f;
+        }
+        float4 row[NB];
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+          row[i] = __ldg(reinterpret_cast<const float4*>(a.Ub + (size_t)b[i] * a.R) + sub);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          if (i < nb) {
+            t.x = fmaf(v[i], row[i].x, t.x);
+            t.y = fmaf(v[i], row[i].y, t.y);
+            t.z = fmaf(v[i], row[i].z, t.z);
+            t.w = fmaf(v[i], row[i].w, t.w);
+            const int64_t kk = k + i + 1;
+            const bool fiber_done = kk == fib_end;
+            if (fiber_done || kk == kend) {
+              acc.x = fmaf(ua.x, t.x, acc.x);
+              acc.y = fmaf(ua.y, t.y, acc.y);
+              acc.z = fmaf(ua.z, t.z, acc.z);
+              acc.w = fmaf(ua.w, t.w, acc.w);
+              t = zero4;
+              if (fiber_done) {
+                ++f;
+                fib_end = nf_end;
+                ua = n_ua;
+                if (f + 1 < a.n_fibers) {
+                  nf_end = __ldg(a.fib_ptr + f + 2);
+                  n_ua = __ldg(reinterpret_cast<const float4*>(
+                                   a.Ua + (size_t)__ldg(a.fib_ids + f + 1) * a.R) + sub);
+                }
+              }
+              const bool root_done = kk == root_end;
+              if (root_done || kk == kend) {
+                if (priv) {
+                  float* r = reinterpret_cast<float*>(win + (s - wlo) * G + sub);
+                  atomicAdd(r + 0, acc.x);
+                  atomicAdd(r + 1, acc.y);
+                  atomicAdd(r + 2, acc.z);
+                  atomicAdd(r + 3, acc.w);
+                } else {
+                  const uint32_t ri = __ldg(a.root_ids + s);
+                  atomicAdd(reinterpret_cast<float4*>(a.M + (size_t)ri * a.R) + sub, acc);
+                }
+                acc = zero4;
+                if (root_done && ++s < a.n_roots) root_end = __ldg(a.root_ptr + s + 1);
+              }
             }
-            acc = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (root_done && ++s < a.n_roots) root_end = __ldg(a.root_ptr + s + 1);
           }
         }
+        k += nb;
       }
     }
     if (priv) {
@@ -516,7 +548,7 @@ template <int G>
 void launch_csf3(tsr_ctx* ctx, cudaStream_t s, const Csf3Args& a) {
   const int64_t gpc = CSF_THREADS / G;
   const int64_t blocks = ceil_div(a.n_chunks, gpc);
-  const int64_t cap = (int64_t)std::max(1, ctx->sm_count - ctx->reserve_sms) * 6;
+  const int64_t cap = (int64_t)std::max(1, ctx->sm_count - ctx->reserve_sms) * 4;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min(blocks, cap));
   csf3_mttkrp_kernel<G><<<grid, CSF_THREADS, sizeof(float4) * CSF_WMAX * G, s>>>(a);
 }

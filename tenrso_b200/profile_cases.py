@@ -59,7 +59,35 @@ def case_cp_als(args):
     print("cp_als", args.precision, shape, "rank", args.rank, "fit", fit, "iters", it)
 
 
-CASES = {"mttkrp": case_mttkrp, "cp_als": case_cp_als}
+def case_csf_mttkrp(args):
+    """CSF MTTKRP on the seeded Zipf(1.2) tensor (device-drawn, merged)."""
+    import torch
+
+    import tenrso_b200 as tb
+    ctx = _ctx()
+    shape = tuple(args.shape) if len(args.shape) == 3 and args.shape != [256, 256, 256] \
+        else (100000, 80000, 10000)
+    cap = 12 * args.nnz
+    d_idx = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_val = torch.empty(cap, dtype=torch.float32, device="cuda")
+    n_raw = tb.synth_zipf_coo_dev(shape, args.nnz, 0xC3, d_idx.data_ptr(), d_val.data_ptr(), cap,
+                                  ctx=ctx)
+    n = tb.coo_deduplicate_dev(d_idx.data_ptr(), d_val.data_ptr(), n_raw, shape, ctx=ctx)
+    sp = tb.SparseTensor(ctx=ctx, d_indices=d_idx.data_ptr(), d_values=d_val.data_ptr(), nnz=n,
+                         shape=shape)
+    del d_idx, d_val
+    g = torch.Generator(device="cuda").manual_seed(1)
+    fs = [torch.rand(m, args.rank, device="cuda", generator=g) for m in shape]
+    M = torch.empty(shape[args.mode], args.rank, device="cuda")
+    for _ in range(args.warmup + args.launches):
+        sp.mttkrp_dev([f.data_ptr() for f in fs], args.rank, args.mode, M.data_ptr())
+    torch.cuda.synchronize()
+    print("csf_mttkrp", shape, "nnz", n, "rank", args.rank, "mode", args.mode,
+          "checksum", float(M.double().sum()), sp.info(args.mode))
+    sp.close()
+
+
+CASES = {"mttkrp": case_mttkrp, "cp_als": case_cp_als, "csf_mttkrp": case_csf_mttkrp}
 
 
 def main(argv=None):
@@ -72,6 +100,7 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--launches", type=int, default=1)
+    ap.add_argument("--nnz", type=int, default=20_000_000)
     args = ap.parse_args(argv)
     CASES[args.case](args)
 
