@@ -128,6 +128,24 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
                                int mode, int precision, int iters, int flush_l2,
                                double* ms_per_launch, int64_t* splits_out);
 
+/* Allocation-free MTTKRP of mode 0 (FP32 split-K path). No tenrso
+ * counterpart: it exists for callers that cannot call cudaMalloc (code whose
+ * device memory is owned by another framework's caching allocator, or code
+ * that enqueues work during CUDA-graph stream capture). It takes a stream
+ * instead of a tsr_ctx and keeps its split partials in a fixed 16 MiB
+ * device array that every GPU loading the library holds until exit; it calls
+ * no cudaMalloc/cudaFree. Device pointers, row-major layouts as
+ * tsr_mttkrp_dev_f32; needs prod(shape[1:]) % 4 == 0 and a 16-byte aligned
+ * tensor, and rejects with TSR_E_UNSUPPORTED any problem whose split partials
+ * (shape[0] x rank x the kernel's split count) exceed the array's 4 Mi
+ * floats. The first call on a device
+ * resolves the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. All calls share the array, so calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
+                                 const int64_t* shape, const float* const* d_factors,
+                                 int64_t rank, float* d_out);
+
 /* ---- CP-ALS: crates/tenrso-decomp/src/cp/core.rs:91-214 -----------------
  * Same loop, validation (rank in [1, min I_n], tol in [0,1)), fit, oscillation
  * and convergence rules. init_factors: concatenated row-major I_0xR, I_1xR, ...

@@ -48,6 +48,7 @@ SIGNATURES = {
     "tsr_mttkrp_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, C.c_int, P]),
     "tsr_profile_mttkrp_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.POINTER(C.c_double), PI64]),
+    "tsr_mttkrp_mode0_noalloc_f32": (C.c_int, [P, P, C.c_int, P, P, I64, P]),
     "tsr_cp_als_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_uint64,
                                  C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
     "tsr_cp_als_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_int,
