@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sparse", action="store_true")
     ap.add_argument("--sparse-nnz", type=int, default=50_000_000)
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -217,6 +218,82 @@ def run_sparse(tb, torch, ctx, stream, args, world, dist):
             "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / 6549.4}
 
 
+AD_SHAPE = (128, 96, 64, 48)
+AD_RANK = 32
+AD_REG = 1e-3
+AD_SEED = 0xC5
+
+
+def run_adjoint(tb, torch, ctx, stream, args, world, dist, rank):
+    """Loss + gradient of ||X - [[A,B,C,D]]||^2 + 1e-3 sum ||U||^2 at
+    128x96x64x48, R=32 (seeded N(0,1) target and factors): the Gram form on a
+    prepared tensor (one MTTKRP of X per mode), in FP32 and BF16x3, and the
+    recompute form (GPU residual G = 2(Xhat - X), then the reconstruction
+    adjoint on G)."""
+    rng = np.random.default_rng(AD_SEED)
+    X = rng.standard_normal(AD_SHAPE).astype(np.float32)
+    fs = [rng.standard_normal((n, AD_RANK)).astype(np.float32) for n in AD_SHAPE]
+    dX = torch.from_numpy(X).cuda()
+    dF = [torch.from_numpy(f).cuda() for f in fs]
+    dGr = [torch.empty_like(f) for f in dF]
+    fptr = [f.data_ptr() for f in dF]
+    gptr = [g.data_ptr() for g in dGr]
+    steps = max(5, args.steps)
+    out = {"workload": "CP loss+gradient 128x96x64x48, rank 32, reg 1e-3",
+           "bytes_alg_per_eval": 4 * 4 * X.size}
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, (ctx.launches - l0) // steps
+
+    for prec in ("fp32", "bf16x3"):
+        d = tb.DenseTensor(dX.data_ptr(), AD_SHAPE, prec, ctx=ctx)
+        ms, launches = timed(lambda: d.loss_grad_dev(fptr, AD_RANK, AD_REG, gptr,
+                                                     want_loss=False))
+        loss = d.loss_grad_dev(fptr, AD_RANK, AD_REG, gptr)
+        d.close()
+        out[f"gram_form_{prec}"] = {
+            "evals_per_s": world * 1e3 / ms, "ms_per_eval": ms, "loss": loss,
+            "launches_per_eval": launches,
+            "achieved_gbs": out["bytes_alg_per_eval"] / (ms * 1e-3) / 1e9}
+    dG = torch.empty_like(dX)
+
+    def recompute():
+        tb.cp_residual_dev(dX.data_ptr(), AD_SHAPE, fptr, AD_RANK, dG.data_ptr(), 2.0,
+                           want_sq=False, ctx=ctx)
+        tb.reconstruction_grad_dev(dG.data_ptr(), AD_SHAPE, fptr, AD_RANK, gptr, ctx=ctx)
+
+    ms, launches = timed(recompute)
+    out["recompute_form_fp32"] = {"evals_per_s": world * 1e3 / ms, "ms_per_eval": ms,
+                                  "launches_per_eval": launches}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        t0 = time.perf_counter()
+        orc.cp_loss_grad_vjp(X, fs, AD_REG)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "evals/s", "cores": orc.num_threads(),
+                               "kind": "port",
+                               "sample": "one FP64 CPU VJP: restated cp_reconstruct, "
+                                         "G = 2(Xhat - X), restated CpReconstructionGrad"}
+    return out
+
+
 def run_ours(args):
     import torch
     import tenrso_b200 as tb
@@ -335,6 +412,8 @@ def run_ours(args):
            "api": "tsr_cp_als_f32 (host pointers)"}
 
     sparse = None if args.no_sparse else run_sparse(tb, torch, ctx, stream, args, world, dist)
+    adjoint = None if args.no_adjoint else run_adjoint(tb, torch, ctx, stream, args, world, dist,
+                                                       rank)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -368,7 +447,7 @@ def run_ours(args):
             "fit_mixed": fit_mixed, "fit_fp32": fit_fp32,
             "fit_abs_diff": abs(fit_mixed - fit_fp32),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": int(launches), "sparse": sparse,
+            "gpu_launches": int(launches), "sparse": sparse, "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -223,6 +223,51 @@ int tsr_cp_als_sparse_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, 
                               double tol, const float* d_init, double time_limit_s,
                               float* d_out_factors, tsr_cp_info* info);
 
+/* ---- CP reconstruction and its adjoint ----------------------------------
+ * tenrso_kernels::cp_reconstruct (crates/tenrso-kernels/src/outer.rs:223-274):
+ * out (row-major, prod of factor_rows) = sum_r w_r U_0[:,r] o ... o U_{N-1}[:,r].
+ * weights may be NULL (all ones). Errors as outer.rs:231-255. */
+int tsr_cp_reconstruct_f32(tsr_ctx* ctx, const float* const* factors, int n_factors,
+                           const int64_t* factor_rows, const int64_t* factor_cols,
+                           const float* weights, int64_t n_weights, float* out);
+int tsr_cp_reconstruct_dev_f32(tsr_ctx* ctx, const float* const* d_factors, int ndim,
+                               const int64_t* shape, int64_t rank, const float* d_weights,
+                               float* d_out);
+/* Forward of the reconstruction loss (no tenrso counterpart): d_out = alpha *
+ * (Xhat - X) (alpha = 2 gives dL/dXhat of ||X - Xhat||^2) and, when sq_err is
+ * not NULL, *sq_err = sum (Xhat - X)^2 in FP64 (the call then synchronizes).
+ * d_out may alias d_tensor. */
+int tsr_cp_residual_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                            const float* const* d_factors, int64_t rank, const float* d_weights,
+                            float alpha, float* d_out, double* sq_err);
+/* CpReconstructionGrad::compute_factor_gradients (crates/tenrso-ad/src/grad.rs:81-120),
+ * the VjpOp rule of the reconstruction: out_grads[n] (shape[n] x rank) =
+ * unfold(G, n) . KR_{m != n}(U_m) . diag(weights), computed as an MTTKRP of G
+ * whose Khatri-Rao rows are never stored. Errors as grad.rs:84-91, 137-139. */
+int tsr_cp_reconstruction_grad_f32(tsr_ctx* ctx, const float* grad_output, int grad_ndim,
+                                   const int64_t* shape, const float* const* factors,
+                                   int n_factors, const int64_t* factor_rows,
+                                   const int64_t* factor_cols, const float* weights,
+                                   int64_t n_weights, int precision, float* const* out_grads);
+int tsr_cp_reconstruction_grad_dev_f32(tsr_ctx* ctx, const float* d_grad_output, int ndim,
+                                       const int64_t* shape, const float* const* d_factors,
+                                       int64_t rank, const float* d_weights, int precision,
+                                       float* const* d_out_grads);
+/* A device tensor prepared for repeated MTTKRPs (no tenrso counterpart): its
+ * per-mode unfoldings in `precision` are built once and owned by the object;
+ * d_tensor stays the caller's and must not change while the object lives. */
+typedef struct tsr_dense tsr_dense;
+int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                             int precision, tsr_dense** out);
+int tsr_dense_destroy(tsr_dense* X);
+/* Loss ||X - [[U]]||^2 + reg * sum_n ||U_n||_F^2 and every dL/dU_n (no tenrso
+ * counterpart; the gradient equals grad.rs's rule applied to G = 2(Xhat - X)
+ * plus 2 reg U_n), evaluated through Gram identities without forming Xhat:
+ * one MTTKRP of X per mode plus FP64 R x R work. d_grads[n]: shape[n] x rank.
+ * loss may be NULL (no synchronization); otherwise the call synchronizes. */
+int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* const* d_factors,
+                             int64_t rank, double reg, float* const* d_grads, double* loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -560,6 +560,42 @@ void orc_cp_reconstruct_f64(const double* const* U, int ndim, const int64_t* sha
   }
 }
 
+// Sum over the slice {i_mode = index} of (X - Xhat)^2 in FP64, with Xhat the
+// reconstruction of outer.rs:223-274 (no weights). Perturbing U_mode[index, r]
+// changes Xhat only on this slice, so central differences of the loss
+// ||X - Xhat||^2 in that entry need only this slice (test infrastructure for
+// the finite-difference check of the reconstruction gradient, grad.rs:81-120).
+double orc_cp_slice_sqerr_f64(const double* X, int ndim, const int64_t* shape,
+                              const double* const* U, int64_t R, int mode, int64_t index) {
+  int64_t total = 1;
+  for (int d = 0; d < ndim; ++d) total *= shape[d];
+  const int64_t n_slice = total / shape[mode];
+  double acc = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : acc)
+  for (int64_t t = 0; t < n_slice; ++t) {
+    // decode t over the other modes (last fastest), then place `index`
+    std::vector<int64_t> ix(ndim);
+    int64_t rem = t;
+    for (int d = ndim - 1; d >= 0; --d) {
+      if (d == mode) continue;
+      ix[d] = rem % shape[d];
+      rem /= shape[d];
+    }
+    ix[mode] = index;
+    int64_t lin = 0;
+    for (int d = 0; d < ndim; ++d) lin = lin * shape[d] + ix[d];
+    double s = 0.0;
+    for (int64_t r = 0; r < R; ++r) {
+      double p = 1.0;
+      for (int d = 0; d < ndim; ++d) p *= U[d][ix[d] * R + r];
+      s += p;
+    }
+    const double e = X[lin] - s;
+    acc += e * e;
+  }
+  return acc;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

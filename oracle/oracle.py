@@ -56,6 +56,8 @@ def lib():
         L.orc_csf_from_coo_f32.argtypes = [P, P, I64, C.c_int, P, P, P, P, P]
         L.orc_coo_mttkrp_f64.argtypes = [P, P, I64, C.c_int, P, P, I64, C.c_int, P]
         L.orc_cp_reconstruct_f64.argtypes = [P, C.c_int, P, I64, P, P]
+        L.orc_cp_slice_sqerr_f64.argtypes = [P, C.c_int, P, P, I64, C.c_int, I64]
+        L.orc_cp_slice_sqerr_f64.restype = C.c_double
         L.orc_num_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -223,6 +225,44 @@ def cp_reconstruction_grad(factors, grad_output, weights=None):
             g = g * np.asarray(weights, dtype=np.float64)[None, :]
         out.append(g)
     return out
+
+
+def cp_loss_grad_vjp(X, factors, reg: float):
+    """CPU VJP of L = ||X - [[U]]||^2 + reg * sum ||U_n||^2 in FP64: restated
+    cp_reconstruct, G = 2 (Xhat - X), restated CpReconstructionGrad on G, plus
+    2 reg U_n. Returns (loss, [dL/dU_n])."""
+    Xd = np.asarray(X, dtype=np.float64)
+    fs = [np.asarray(f, dtype=np.float64) for f in factors]
+    Xh = cp_reconstruct(fs)
+    D = Xh - Xd
+    loss = float(np.sum(D * D) + reg * sum(float(np.sum(f * f)) for f in fs))
+    grads = cp_reconstruction_grad(fs, 2.0 * D)
+    return loss, [g + 2.0 * reg * f for g, f in zip(grads, fs)]
+
+
+def cp_slice_sqerr(X, factors, mode: int, index: int) -> float:
+    """sum over the slice i_mode = index of (X - Xhat)^2, FP64."""
+    Xd = np.ascontiguousarray(X, dtype=np.float64)
+    fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    shp = np.asarray(Xd.shape, dtype=np.int64)
+    return float(lib().orc_cp_slice_sqerr_f64(_ptr(Xd), Xd.ndim, _ptr(shp), _ptr_array(fs), fs[0].shape[1], mode, index))
+
+
+def fd_grad_entries(X, factors, reg: float, mode: int, entries, h: float = 1e-6):
+    """FP64 central differences of L = ||X - [[U]]||^2 + reg sum ||U||^2 in the
+    entries (i, r) of U_mode, each from the loss restricted to slice i (the
+    only part of ||X - Xhat||^2 the entry changes)."""
+    fs = [np.array(f, dtype=np.float64) for f in factors]
+    out = []
+    for i, r in entries:
+        u0 = fs[mode][i, r]
+        fs[mode][i, r] = u0 + h
+        lp = cp_slice_sqerr(X, fs, mode, i) + reg * (u0 + h) ** 2
+        fs[mode][i, r] = u0 - h
+        lm = cp_slice_sqerr(X, fs, mode, i) + reg * (u0 - h) ** 2
+        fs[mode][i, r] = u0
+        out.append((lp - lm) / (2.0 * h))
+    return np.array(out)
 
 
 def csf_to_coo(fptr, fids, vals, mode_order):

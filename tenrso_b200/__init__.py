@@ -33,4 +33,15 @@ from .sparse import (  # noqa: F401
     synth_zipf_coo_dev,
 )
 
+from .adjoint import (  # noqa: F401
+    CpReconstructionGrad,
+    CpReconstructionOp,
+    DenseTensor,
+    cp_loss_grad,
+    cp_reconstruct,
+    cp_reconstruct_dev,
+    cp_residual_dev,
+    reconstruction_grad_dev,
+)
+
 __version__ = "0.1.0"

@@ -71,6 +71,16 @@ SIGNATURES = {
                                         P, C.POINTER(CpInfo)]),
     "tsr_cp_als_sparse_dev_f32": (C.c_int, [P, P, I64, C.c_int, C.c_double, P, C.c_double, P,
                                             C.POINTER(CpInfo)]),
+    "tsr_cp_reconstruct_f32": (C.c_int, [P, P, C.c_int, P, P, P, I64, P]),
+    "tsr_cp_reconstruct_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, P, P]),
+    "tsr_cp_residual_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, P, C.c_float, P,
+                                          C.POINTER(C.c_double)]),
+    "tsr_cp_reconstruction_grad_f32": (C.c_int, [P, P, C.c_int, P, P, C.c_int, P, P, P, I64,
+                                                 C.c_int, P]),
+    "tsr_cp_reconstruction_grad_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, P, C.c_int, P]),
+    "tsr_dense_create_dev_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(P)]),
+    "tsr_dense_destroy": (C.c_int, [P]),
+    "tsr_cp_loss_grad_dev_f32": (C.c_int, [P, P, P, I64, C.c_double, P, C.POINTER(C.c_double)]),
 }
 
 _lib = None

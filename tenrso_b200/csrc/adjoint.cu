@@ -1,0 +1,639 @@
+// CP reconstruction, its adjoint, and the loss/gradient of a CP model.
+//
+//   tenrso_kernels::cp_reconstruct                  crates/tenrso-kernels/src/outer.rs:223-274
+//     Xhat = sum_r w_r U_0[:, r] o U_1[:, r] o ... o U_{N-1}[:, r]
+//   CpReconstructionGrad::compute_factor_gradients  crates/tenrso-ad/src/grad.rs:81-120
+//     dL/dU_n = unfold(G, n) . KR_{m != n}(U_m) . diag(w),  G = dL/dXhat
+//   that is, the MTTKRP of G; the Khatri-Rao rows are formed on the fly by the
+//   MTTKRP kernels and never stored (grad.rs:128-150 materialises them).
+//
+// The loss/gradient entry evaluates  L = ||X - [[U]]||^2 + reg * sum_n ||U_n||^2
+// and all dL/dU_n without forming Xhat, from the Gram identities
+//   ||Xhat||^2   = sum_{r,s} prod_n (U_n^T U_n)[r, s]
+//   <X, Xhat>    = sum_{i,r} MTTKRP(X, 0)[i, r] U_0[i, r]
+//   dL/dU_n      = 2 (U_n H_n - MTTKRP(X, n)) + 2 reg U_n,  H_n = *_{m != n} U_m^T U_m
+// with the Grams, H_n, the loss and the U_n H_n product in FP64.
+#include <cstring>
+
+#include "als.cuh"
+#include "dense.cuh"
+
+// A dense tensor prepared for repeated MTTKRPs: its per-mode unfoldings (in
+// the precision the MTTKRP reads) are built once and kept in HBM. The tensor
+// itself stays the caller's and must not change while the object is in use.
+struct tsr_dense {
+  int ndim = 0;
+  int64_t shape[tsr::kMaxModes] = {};
+  int precision = 0;
+  int device = 0;
+  const float* dX = nullptr;
+  void* owned[2 * tsr::kMaxModes] = {};
+  tsr::ModeOperand ops[tsr::kMaxModes];
+  double* d_scalars = nullptr;  // [0] ||X||^2, [1] <X, Xhat>, [2] loss
+};
+
+namespace tsr {
+
+namespace {
+
+constexpr int RC_THREADS = 256;
+constexpr int RC_TILE = 64;   // output tile: 64 rows x 64 columns, 4 x 4 per thread
+constexpr int RC_CHUNK = 32;  // rank columns staged in shared memory per pass
+
+// The row-major output seen as a P x Lc matrix: rows run over modes
+// [0, split), columns over the trailing modes [split, N) (the last fastest),
+// so element (p, c) sits at p * Lc + c. Both operands of the tile product are
+// Khatri-Rao rows built from the factors inside the kernel.
+struct ReconArgs {
+  FactorTable ft;
+  int ndim;
+  int split;
+  int R;
+  int64_t P, Lc;
+  const float* w;    // weights (R) or null for all ones
+  const float* X;    // residual mode: the target tensor
+  float* out;        // Xhat, or alpha * (Xhat - X)
+  float alpha;
+  double* sq_err;    // residual mode: sum of (Xhat - X)^2 added here
+};
+
+// Offsets (element index * R) of one KR row's factor entries, modes [m0, m1).
+__device__ __forceinline__ void kr_offsets(const ReconArgs& a, int m0, int m1, int64_t idx,
+                                           int64_t* off) {
+  for (int m = m1 - 1; m >= m0; --m) {
+    const int64_t n = a.ft.rows[m];
+    const int64_t q = idx / n;
+    off[m] = (idx - q * n) * a.R;
+    idx = q;
+  }
+}
+
+template <bool RESIDUAL, bool VEC4>
+__global__ void __launch_bounds__(RC_THREADS)
+reconstruct_kernel(ReconArgs a) {
+  __shared__ __align__(16) float Ws[RC_CHUNK][RC_TILE];  // row operand, rank-major
+  __shared__ __align__(16) float Vs[RC_CHUNK][RC_TILE];  // column operand, rank-major
+  __shared__ int64_t row_off[kMaxModes][RC_TILE];
+  __shared__ int64_t col_off[kMaxModes][RC_TILE];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int64_t p0 = (int64_t)blockIdx.y * RC_TILE;
+  const int64_t c0 = (int64_t)blockIdx.x * RC_TILE;
+  if (threadIdx.x < RC_TILE) {
+    int64_t off[kMaxModes];
+    const int64_t p = p0 + threadIdx.x;
+    kr_offsets(a, 0, a.split, p < a.P ? p : 0, off);
+    for (int m = 0; m < a.split; ++m) row_off[m][threadIdx.x] = off[m];
+  } else if (threadIdx.x < 2 * RC_TILE) {
+    int64_t off[kMaxModes];
+    const int64_t c = c0 + threadIdx.x - RC_TILE;
+    kr_offsets(a, a.split, a.ndim, c < a.Lc ? c : 0, off);
+    for (int m = a.split; m < a.ndim; ++m) col_off[m][threadIdx.x - RC_TILE] = off[m];
+  }
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int r0 = 0; r0 < a.R; r0 += RC_CHUNK) {
+    __syncthreads();
+    // stage KR entries: thread e covers (row/col i, rank r) with r fastest
+    for (int e = threadIdx.x; e < RC_TILE * RC_CHUNK; e += RC_THREADS) {
+      const int i = e / RC_CHUNK, r = e % RC_CHUNK;
+      const int rr = r0 + r;
+      float wv = 0.f, vv = 0.f;
+      if (rr < a.R) {
+        wv = (p0 + i < a.P) ? (a.w ? __ldg(a.w + rr) : 1.f) : 0.f;
+        for (int m = 0; m < a.split; ++m) wv *= __ldg(a.ft.ptr[m] + row_off[m][i] + rr);
+        vv = (c0 + i < a.Lc) ? 1.f : 0.f;
+        for (int m = a.split; m < a.ndim; ++m) vv *= __ldg(a.ft.ptr[m] + col_off[m][i] + rr);
+      }
+      Ws[r][i] = wv;
+      Vs[r][i] = vv;
+    }
+    __syncthreads();
+    const int rn = a.R - r0 < RC_CHUNK ? a.R - r0 : RC_CHUNK;
+#pragma unroll 8
+    for (int r = 0; r < rn; ++r) {
+      const float4 wv = *reinterpret_cast<const float4*>(&Ws[r][ty * 4]);
+      const float4 vv = *reinterpret_cast<const float4*>(&Vs[r][tx * 4]);
+      const float wa[4] = {wv.x, wv.y, wv.z, wv.w};
+      const float va[4] = {vv.x, vv.y, vv.z, vv.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(wa[i], va[j], acc[i][j]);
+    }
+  }
+  double sq = 0.0;
+  const int64_t c = c0 + tx * 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t p = p0 + ty * 4 + i;
+    if (p >= a.P) continue;
+    const int64_t base = p * a.Lc + c;
+    if (VEC4 && c + 3 < a.Lc) {
+      float4 v = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+      if (RESIDUAL) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(a.X + base));
+        const float d0 = v.x - x.x, d1 = v.y - x.y, d2 = v.z - x.z, d3 = v.w - x.w;
+        sq += (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2 + (double)d3 * d3;
+        v = make_float4(a.alpha * d0, a.alpha * d1, a.alpha * d2, a.alpha * d3);
+      }
+      __stcs(reinterpret_cast<float4*>(a.out + base), v);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (c + j >= a.Lc) break;
+        float v = acc[i][j];
+        if (RESIDUAL) {
+          const float d = v - __ldg(a.X + base + j);
+          sq += (double)d * d;
+          v = a.alpha * d;
+        }
+        a.out[base + j] = v;
+      }
+    }
+  }
+  if (RESIDUAL) {
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(a.sq_err, sq);
+  }
+}
+
+__device__ __forceinline__ double sym_at(const double* g, int R, int a, int c) {
+  return a <= c ? g[a * R + c] : g[c * R + a];
+}
+
+// Gradient rows of one mode in Gram form:
+//   out[i, :] = 2 (U[i, :] H - M[i, :] + reg U[i, :]),  H = *_{m != mode} Gram_m
+// where M is the sum of the split MTTKRP partials. Mode 0 also accumulates
+// <M, U> (= <X, Xhat>) into scal[1]. Shared (FP64): H (R x R), M (rows x R),
+// and the per-group partial sums: `groups` threads share one element of M and
+// each sums a strided subset of the splits with 8 loads in flight.
+__global__ void __launch_bounds__(256)
+gram_grad_kernel(const double* __restrict__ grams, int ndim, int mode,
+                 const float* __restrict__ partials, int splits, int64_t rows, int R,
+                 int rows_per_cta, const float* __restrict__ U, double reg,
+                 float* __restrict__ out, double* scal) {
+  extern __shared__ double sh[];
+  const int RR = R * R;
+  double* H = sh;
+  double* Ms = sh + RR;
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
+    const int a = e / R, c = e % R;
+    double h = 1.0;
+    for (int m = 0; m < ndim; ++m)
+      if (m != mode) h *= sym_at(grams + (int64_t)m * RR, R, a, c);
+    H[e] = h;
+  }
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+  const int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
+  const int64_t pstride = rows * R;
+  const int ne = nr * R;
+  const int full = rows_per_cta * R;
+  const int groups = full >= (int)blockDim.x ? 1 : (int)blockDim.x / full;
+  double* red = Ms + full;  // [groups][ne]
+  for (int t = threadIdx.x; t < ne * groups; t += blockDim.x) {
+    const int e = t % ne, g = t / ne;
+    const float* p = partials + r0 * R + e;
+    double s = 0.0;
+    int q = g;
+    for (; q + 7 * groups < splits; q += 8 * groups) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = __ldg(p + (int64_t)(q + u * groups) * pstride);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += (double)v[u];
+    }
+    for (; q < splits; q += groups) s += (double)__ldg(p + (int64_t)q * pstride);
+    red[g * ne + e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    double s = 0.0;
+    for (int g = 0; g < groups; ++g) s += red[g * ne + e];
+    Ms[e] = s;
+  }
+  __syncthreads();
+  double ip = 0.0;
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    const int i = e / R, c = e % R;
+    const float* urow = U + (r0 + i) * R;
+    double s0 = 0.0, s1 = 0.0;
+    int k = 0;
+    for (; k + 2 <= R; k += 2) {
+      s0 += (double)__ldg(urow + k) * H[k * R + c];
+      s1 += (double)__ldg(urow + k + 1) * H[(k + 1) * R + c];
+    }
+    if (k < R) s0 += (double)__ldg(urow + k) * H[k * R + c];
+    const double u = (double)__ldg(urow + c);
+    out[(r0 + i) * R + c] = (float)(2.0 * ((s0 + s1) - Ms[e] + reg * u));
+    ip += Ms[e] * u;
+  }
+  if (mode == 0) {
+    for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(scal + 1, ip);
+  }
+}
+
+// loss = ||X||^2 - 2 <X, Xhat> + sum_{r,s} prod_n Gram_n[r, s] + reg sum_n tr(Gram_n)
+__global__ void gram_loss_kernel(const double* __restrict__ grams, int ndim, int R, double reg,
+                                 double* scal) {
+  const int RR = R * R;
+  double s = 0.0;
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
+    const int a = e / R, c = e % R;
+    double h = 1.0, tr = 0.0;
+    for (int m = 0; m < ndim; ++m) {
+      const double g = sym_at(grams + (int64_t)m * RR, R, a, c);
+      h *= g;
+      if (a == c) tr += g;
+    }
+    s += h + reg * tr;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+  scal[2] = scal[0] - 2.0 * scal[1] + t;
+}
+
+int64_t prod_range(const int64_t* shape, int m0, int m1) {
+  int64_t p = 1;
+  for (int m = m0; m < m1; ++m) p *= shape[m];
+  return p;
+}
+
+// Shared validation of tenrso's cp_reconstruct (outer.rs:231-255).
+int validate_reconstruct(int n_factors, const int64_t* fcols, int64_t n_weights, bool has_w) {
+  if (n_factors <= 0)
+    return fail(TSR_E_SHAPE, "Need at least one factor matrix for CP reconstruction");
+  const int64_t R = fcols[0];
+  for (int i = 0; i < n_factors; ++i)
+    if (fcols[i] != R)
+      return fail(TSR_E_RANK_MISMATCH, "Factor %d has %lld columns, expected %lld", i,
+                  (long long)fcols[i], (long long)R);
+  if (has_w && n_weights != R)
+    return fail(TSR_E_SHAPE, "Weights length %lld must match rank %lld", (long long)n_weights,
+                (long long)R);
+  if (n_factors > kMaxModes)
+    return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", n_factors,
+                kMaxModes);
+  return TSR_OK;
+}
+
+}  // namespace
+
+void init_adjoint_attributes() {
+  cudaFuncSetAttribute(gram_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+// Xhat (or alpha * (Xhat - X) with sum of squares) on the context's stream.
+int launch_reconstruct(tsr_ctx* ctx, const FactorTable& ft, int ndim, int R, const float* w,
+                       const float* X, float alpha, double* sq_err, float* out) {
+  ReconArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ft = ft;
+  a.ndim = ndim;
+  a.R = R;
+  a.w = w;
+  a.X = X;
+  a.out = out;
+  a.alpha = alpha;
+  a.sq_err = sq_err;
+  int64_t shape[kMaxModes];
+  for (int m = 0; m < ndim; ++m) shape[m] = ft.rows[m];
+  // the fewest trailing modes that fill a 64-wide column tile
+  int split = ndim - 1;
+  while (split > 0 && prod_range(shape, split, ndim) < RC_TILE) --split;
+  if (prod_range(shape, split, ndim) < RC_TILE) split = 0;
+  a.split = split;
+  a.P = prod_range(shape, 0, split);
+  a.Lc = prod_range(shape, split, ndim);
+  if (a.P == 0 || a.Lc == 0) return TSR_OK;
+  const int64_t gy = ceil_div(a.P, RC_TILE);
+  if (gy > 65535) {
+    // fold excess rows into columns: keep the grid's y extent legal
+    while (split > 0 && ceil_div(prod_range(shape, 0, split), RC_TILE) > 65535) --split;
+    a.split = split;
+    a.P = prod_range(shape, 0, split);
+    a.Lc = prod_range(shape, split, ndim);
+  }
+  const int64_t gx = ceil_div(a.Lc, RC_TILE);
+  if (gx > 0x7fffffffLL)
+    return fail(TSR_E_UNSUPPORTED, "tensor too large for the reconstruction kernel");
+  const dim3 grid((unsigned)gx, (unsigned)ceil_div(a.P, RC_TILE));
+  const bool vec = (a.Lc % 4 == 0) && !((uintptr_t)out & 15) && !((uintptr_t)X & 15);
+  if (X) {
+    if (vec) reconstruct_kernel<true, true><<<grid, RC_THREADS, 0, ctx->stream>>>(a);
+    else reconstruct_kernel<true, false><<<grid, RC_THREADS, 0, ctx->stream>>>(a);
+  } else {
+    if (vec) reconstruct_kernel<false, true><<<grid, RC_THREADS, 0, ctx->stream>>>(a);
+    else reconstruct_kernel<false, false><<<grid, RC_THREADS, 0, ctx->stream>>>(a);
+  }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+namespace {
+
+// dL/dU_n for every mode of a device gradient tensor G (grad.rs:81-120).
+int reconstruction_grad_device(tsr_ctx* ctx, const float* dG, int ndim, const int64_t* shape,
+                               const FactorTable& ft, int R, const float* dw, int precision,
+                               float* const* d_out) {
+  for (int n = 0; n < ndim; ++n) {
+    if (shape[n] == 0) continue;
+    if (numel(ndim, shape) == 0 || R == 0) {
+      TSR_CUDA(cudaMemsetAsync(d_out[n], 0, sizeof(float) * shape[n] * R, ctx->stream));
+      continue;
+    }
+    ModeOperand op;
+    TSR_TRY(prepare_mode(ctx, dG, ndim, shape, n, precision, 0, &op));
+    float* partials;
+    int splits;
+    TSR_TRY(run_mttkrp_partials(ctx, op, ft, R, precision, &partials, &splits));
+    TSR_TRY(launch_mttkrp_reduce_scaled(ctx, partials, splits, shape[n], R, dw, d_out[n]));
+  }
+  return TSR_OK;
+}
+
+int validate_grad(int g_ndim, const int64_t* shape, int n_factors, const int64_t* frows,
+                  const int64_t* fcols) {
+  // grad.rs:84-91
+  if (g_ndim != n_factors)
+    return fail(TSR_E_SHAPE, "Gradient rank %d doesn't match number of factors %d", g_ndim,
+                n_factors);
+  // grad.rs:137-139: the Khatri-Rao product of the other factors needs one
+  if (n_factors < 2)
+    return fail(TSR_E_NEED_2_FACTORS, "Need at least one factor for Khatri-Rao product");
+  return validate_mttkrp(g_ndim, shape, n_factors, frows, fcols, 0);
+}
+
+}  // namespace
+
+}  // namespace tsr
+
+using namespace tsr;
+
+extern "C" {
+
+int tsr_cp_reconstruct_f32(tsr_ctx* ctx, const float* const* factors, int n_factors,
+                           const int64_t* factor_rows, const int64_t* factor_cols,
+                           const float* weights, int64_t n_weights, float* out) {
+  if (n_factors > 0 && (!factors || !factor_rows || !factor_cols))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(validate_reconstruct(n_factors, factor_cols, n_weights, weights != nullptr));
+  if (!out) return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(check_ctx(ctx));
+  const int64_t R = factor_cols[0];
+  const int64_t total = numel(n_factors, factor_rows);
+  if (total == 0) return TSR_OK;
+  if (R == 0) {
+    std::memset(out, 0, sizeof(float) * total);
+    return TSR_OK;
+  }
+  FactorTable ft{};
+  TSR_TRY(upload_factors(ctx, n_factors, factor_rows, factors, R, &ft));
+  const float* dw = nullptr;
+  if (weights) {
+    void* p;
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * R, &p));
+    TSR_CUDA(cudaMemcpyAsync(p, weights, sizeof(float) * R, cudaMemcpyHostToDevice, ctx->stream));
+    dw = (const float*)p;
+  }
+  void* dout;
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * total, &dout));
+  TSR_TRY(launch_reconstruct(ctx, ft, n_factors, (int)R, dw, nullptr, 0.f, nullptr,
+                             (float*)dout));
+  TSR_CUDA(cudaMemcpyAsync(out, dout, sizeof(float) * total, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int tsr_cp_reconstruct_dev_f32(tsr_ctx* ctx, const float* const* d_factors, int ndim,
+                               const int64_t* shape, int64_t rank, const float* d_weights,
+                               float* d_out) {
+  if (!d_factors || !shape || !d_out) return fail(TSR_E_INVALID_ARG, "null argument");
+  std::vector<int64_t> cols(ndim > 0 ? ndim : 1, rank);
+  TSR_TRY(validate_reconstruct(ndim, cols.data(), rank, false));
+  TSR_TRY(check_ctx(ctx));
+  const int64_t total = numel(ndim, shape);
+  if (total == 0) return TSR_OK;
+  if (rank == 0) {
+    TSR_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float) * total, ctx->stream));
+    return TSR_OK;
+  }
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = shape[m];
+  }
+  return launch_reconstruct(ctx, ft, ndim, (int)rank, d_weights, nullptr, 0.f, nullptr, d_out);
+}
+
+int tsr_cp_residual_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                            const float* const* d_factors, int64_t rank, const float* d_weights,
+                            float alpha, float* d_out, double* sq_err) {
+  if (!d_tensor || !d_factors || !shape || !d_out) return fail(TSR_E_INVALID_ARG, "null argument");
+  std::vector<int64_t> cols(ndim > 0 ? ndim : 1, rank);
+  TSR_TRY(validate_reconstruct(ndim, cols.data(), rank, false));
+  if (rank <= 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  TSR_TRY(check_ctx(ctx));
+  void* p;
+  TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(double), &p));
+  TSR_CUDA(cudaMemsetAsync(p, 0, sizeof(double), ctx->stream));
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = shape[m];
+  }
+  TSR_TRY(launch_reconstruct(ctx, ft, ndim, (int)rank, d_weights, d_tensor, alpha, (double*)p,
+                             d_out));
+  if (sq_err) {
+    TSR_CUDA(cudaMemcpyAsync(sq_err, p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return TSR_OK;
+}
+
+int tsr_cp_reconstruction_grad_f32(tsr_ctx* ctx, const float* grad_output, int grad_ndim,
+                                   const int64_t* shape, const float* const* factors,
+                                   int n_factors, const int64_t* factor_rows,
+                                   const int64_t* factor_cols, const float* weights,
+                                   int64_t n_weights, int precision, float* const* out_grads) {
+  if (!shape || !grad_output || !out_grads || (n_factors > 0 && (!factors || !factor_rows ||
+                                                                  !factor_cols)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(validate_grad(grad_ndim, shape, n_factors, factor_rows, factor_cols));
+  const int64_t R = factor_cols[0];
+  if (weights && n_weights != R)
+    return fail(TSR_E_SHAPE, "Weights length %lld must match rank %lld", (long long)n_weights,
+                (long long)R);
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  float* dG;
+  TSR_TRY(upload_tensor(ctx, grad_output, grad_ndim, shape, nullptr, &dG));
+  FactorTable ft{};
+  TSR_TRY(upload_factors(ctx, n_factors, shape, factors, R, &ft));
+  const float* dw = nullptr;
+  if (weights && R > 0) {
+    void* p;
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * R, &p));
+    TSR_CUDA(cudaMemcpyAsync(p, weights, sizeof(float) * R, cudaMemcpyHostToDevice, ctx->stream));
+    dw = (const float*)p;
+  }
+  int64_t total = 0;
+  for (int m = 0; m < n_factors; ++m) total += shape[m] * R;
+  void* dout;
+  TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * (total > 0 ? total : 1), &dout));
+  std::vector<float*> outs(n_factors);
+  int64_t off = 0;
+  for (int m = 0; m < n_factors; ++m) {
+    outs[m] = (float*)dout + off;
+    off += shape[m] * R;
+  }
+  TSR_TRY(reconstruction_grad_device(ctx, dG, grad_ndim, shape, ft, (int)R, dw, precision,
+                                     outs.data()));
+  for (int m = 0; m < n_factors; ++m)
+    if (shape[m] * R > 0)
+      TSR_CUDA(cudaMemcpyAsync(out_grads[m], outs[m], sizeof(float) * shape[m] * R,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSR_OK;
+}
+
+int tsr_cp_reconstruction_grad_dev_f32(tsr_ctx* ctx, const float* d_grad_output, int ndim,
+                                       const int64_t* shape, const float* const* d_factors,
+                                       int64_t rank, const float* d_weights, int precision,
+                                       float* const* d_out_grads) {
+  if (!shape || !d_grad_output || !d_factors || !d_out_grads)
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  std::vector<int64_t> cols(ndim > 0 ? ndim : 1, rank);
+  TSR_TRY(validate_grad(ndim, shape, ndim, shape, cols.data()));
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  FactorTable ft{};
+  for (int m = 0; m < ndim; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = shape[m];
+  }
+  return reconstruction_grad_device(ctx, d_grad_output, ndim, shape, ft, (int)rank, d_weights,
+                                    precision, d_out_grads);
+}
+
+int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                             int precision, tsr_dense** out) {
+  if (!d_tensor || !shape || !out) return fail(TSR_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (ndim < 2) return fail(TSR_E_NEED_2_FACTORS, "Need at least 2 factor matrices for MTTKRP");
+  if (ndim > kMaxModes)
+    return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", ndim, kMaxModes);
+  for (int m = 0; m < ndim; ++m)
+    if (shape[m] <= 0) return fail(TSR_E_SHAPE, "mode %d has size %lld", m, (long long)shape[m]);
+  TSR_TRY(check_precision(precision));
+  TSR_TRY(check_ctx(ctx));
+  tsr_dense* d = new tsr_dense();
+  d->ndim = ndim;
+  d->precision = precision;
+  d->device = ctx->device;
+  d->dX = d_tensor;
+  for (int m = 0; m < ndim; ++m) d->shape[m] = shape[m];
+  auto cleanup = [&](int rc) {
+    tsr_dense_destroy(d);
+    return rc;
+  };
+  for (int m = 0; m < ndim; ++m) {
+    size_t ab, bb;
+    mode_operand_bytes(make_unfolding(ndim, shape, m), precision, &ab, &bb);
+    if (ab && cudaMalloc(&d->owned[2 * m], ab) != cudaSuccess)
+      return cleanup(fail(TSR_E_CUDA, "cudaMalloc of %zu bytes failed", ab));
+    if (bb && cudaMalloc(&d->owned[2 * m + 1], bb) != cudaSuccess)
+      return cleanup(fail(TSR_E_CUDA, "cudaMalloc of %zu bytes failed", bb));
+    int rc = prepare_mode_into(ctx, d_tensor, ndim, shape, m, precision, d->owned[2 * m],
+                               d->owned[2 * m + 1], &d->ops[m]);
+    if (rc != TSR_OK) return cleanup(rc);
+  }
+  if (cudaMalloc(&d->d_scalars, 4 * sizeof(double)) != cudaSuccess)
+    return cleanup(fail(TSR_E_CUDA, "cudaMalloc of the loss scalars failed"));
+  cudaError_t e = cudaMemsetAsync(d->d_scalars, 0, 4 * sizeof(double), ctx->stream);
+  if (e != cudaSuccess) return cleanup(fail(TSR_E_CUDA, "%s", cudaGetErrorString(e)));
+  int rc = launch_norm_sq(ctx, ctx->stream, d_tensor, numel(ndim, shape), d->d_scalars);
+  if (rc != TSR_OK) return cleanup(rc);
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cleanup(fail(TSR_E_CUDA, "%s", cudaGetErrorString(e)));
+  *out = d;
+  return TSR_OK;
+}
+
+int tsr_dense_destroy(tsr_dense* d) {
+  if (!d) return TSR_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(d->device);
+  for (void* p : d->owned)
+    if (p) cudaFree(p);
+  if (d->d_scalars) cudaFree(d->d_scalars);
+  cudaSetDevice(prev);
+  delete d;
+  return TSR_OK;
+}
+
+int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* const* d_factors,
+                             int64_t rank, double reg, float* const* d_grads, double* loss) {
+  if (!X || !d_factors || !d_grads) return fail(TSR_E_INVALID_ARG, "null argument");
+  if (rank <= 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  if (rank > kMaxRank)
+    return fail(TSR_E_UNSUPPORTED, "rank %lld exceeds the supported %d", (long long)rank,
+                kMaxRank);
+  TSR_TRY(check_ctx(ctx));
+  if (ctx->device != X->device)
+    return fail(TSR_E_INVALID_ARG, "tensor prepared on device %d, context on device %d",
+                X->device, ctx->device);
+  const int N = X->ndim, R = (int)rank, RR = R * R;
+  FactorTable ft{};
+  for (int m = 0; m < N; ++m) {
+    ft.ptr[m] = d_factors[m];
+    ft.rows[m] = X->shape[m];
+  }
+  void* gp;
+  TSR_TRY(slot_get(ctx, SLOT_GRAMS, sizeof(double) * N * RR, &gp));
+  double* grams = (double*)gp;
+  for (int m = 0; m < N; ++m)
+    TSR_TRY(launch_gram(ctx, ctx->stream, d_factors[m], X->shape[m], R, grams + (size_t)m * RR,
+                        true));
+  TSR_CUDA(cudaMemsetAsync(X->d_scalars + 1, 0, 2 * sizeof(double), ctx->stream));
+  for (int n = 0; n < N; ++n) {
+    float* partials;
+    int splits;
+    TSR_TRY(run_mttkrp_partials(ctx, X->ops[n], ft, R, X->precision, &partials, &splits));
+    const int64_t rows = X->shape[n];
+    const int rpc =
+        (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 2 * ctx->sm_count)));
+    const int full = rpc * R;
+    const int groups = full >= 256 ? 1 : 256 / full;
+    const size_t smem = sizeof(double) * ((size_t)RR + full + (size_t)groups * full);
+    if (smem > 200 * 1024)
+      return fail(TSR_E_UNSUPPORTED, "rank %d too large for the gradient kernel", R);
+    gram_grad_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, ctx->stream>>>(
+        grams, N, n, partials, splits, rows, R, rpc, d_factors[n], reg, d_grads[n],
+        X->d_scalars);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+  }
+  gram_loss_kernel<<<1, 256, 0, ctx->stream>>>(grams, N, R, reg, X->d_scalars);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  if (loss) {
+    TSR_CUDA(cudaMemcpyAsync(loss, X->d_scalars + 2, sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return TSR_OK;
+}
+
+}  // extern "C"

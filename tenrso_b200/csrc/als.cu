@@ -70,7 +70,7 @@ gram_kernel(const float* __restrict__ U, int64_t rows, int R, int64_t rows_per_c
     }
 }
 
-__global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, AlsState* st) {
+__global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* out) {
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   const int64_t n4 = ((uintptr_t)X & 15) ? 0 : n / 4;
   const float4* X4 = reinterpret_cast<const float4*>(X);
@@ -92,7 +92,7 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, AlsState*
   if (threadIdx.x < 32) {
     s = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) atomicAdd(&st->xnorm_sq, s);
+    if (threadIdx.x == 0) atomicAdd(out, s);
   }
 }
 
@@ -465,9 +465,9 @@ int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int 
   return TSR_OK;
 }
 
-int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, AlsState* st) {
+int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, double* out) {
   const int grid = ctx->sm_count * 8;
-  norm_sq_kernel<<<grid, 256, 0, s>>>(X, n, st);
+  norm_sq_kernel<<<grid, 256, 0, s>>>(X, n, out);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

@@ -34,8 +34,8 @@ void init_als_attributes();
 // Upper triangle of U^T U (FP64) accumulated into gram; zero_first memsets it.
 int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int R,
                 double* gram, bool zero_first);
-// ||X||^2 into state->xnorm_sq (which must be zero).
-int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, AlsState* state);
+// ||X||^2 (FP64) added into *out (which the caller zeroes).
+int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, double* out);
 // Hadamard of all Grams except `mode`, its inverse (ridge retry), and the
 // zeroing of gram[mode] (and, when `last`, state->inner) before the solve.
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,

@@ -372,17 +372,7 @@ int check_host_bounds(const int64_t* idx, int64_t nnz, int ndim, const int64_t* 
 }
 
 // ---------------------------------------------------------------------------
-// CSF MTTKRP, 3-way, R % 4 == 0, R <= 128.
-//
-// Groups of G = R/4 lanes own one factor row (one float4 per lane, 128-bit
-// loads). Each group walks a fixed chunk of 256 consecutive entries of the
-// CSF rooted at the output mode: the leaf factor row of every entry is
-// scaled by its value into the fiber sum t; at a fiber end the level-1
-// factor row multiplies t into the root sum; at a root end (or chunk end)
-// the root sum is flushed. The chunks of one CTA are contiguous, so the roots
-// they touch form a window; when the window is small (heavy Zipf roots) it is
-// privatised in shared memory and written back with one atomic per row per
-// CTA. Atomics only ever target output (root-mode) rows.
+// CSF MTTKRP, 3-way (the CSF rooted at the output mode).
 struct Csf3Args {
   const uint32_t* root_ids;
   const uint32_t* root_ptr;
@@ -399,112 +389,174 @@ struct Csf3Args {
   float* M;
 };
 
-constexpr int CSF_THREADS = 256;
-constexpr int CSF_WMAX = 64;  // privatised root rows per CTA window
+// One warp owns a task of 1024 consecutive entries and walks it in batches
+// of BS entries (BS <= 32):
+//   - lane-parallel loads fetch the batch's leaf row offsets and values and
+//     the ends/ids of the next 32 fibers and roots (one batch ahead);
+//   - fiber and root ends inside the batch become warp-uniform bit masks
+//     (__reduce_or_sync);
+//   - lanes form SLOTS = 32 / (R/4) groups of R/4 lanes, each lane holding a
+//     float4 of columns, so one step covers SLOTS entries; the batch's leaf
+//     rows and fiber (level-1) rows are loaded into registers with 128-bit
+//     loads, all in flight together before the first is used (the fiber of
+//     an entry is the popcount of the fiber-end mask below it);
+//   - every entry adds value * leaf row (*) its fiber's row to the open root
+//     sum, with no branch per entry;
+//   - at a root end (or the task end) the slots' partial sums are combined by
+//     shuffles and added to the output row with float4 atomics, the only
+//     atomics in the kernel.
+// The per-entry form equals the fiber-factored form of the reference's
+// MTTKRP definition (sum over entries of v * prod of factor rows); only the
+// fp32 summation order differs.
+constexpr int CSF_WARPS = 8;
 
-template <int G>
-__global__ void __launch_bounds__(CSF_THREADS, 2)
-csf3_mttkrp_kernel(Csf3Args a) {
-  extern __shared__ float4 win[];  // [CSF_WMAX][G]
-  constexpr int GPC = CSF_THREADS / G;
-  constexpr int NB = 8;  // entries whose factor rows are in flight together
-  const int grp = threadIdx.x / G, sub = threadIdx.x % G;
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int64_t blk = blockIdx.x; blk * GPC < a.n_chunks; blk += gridDim.x) {
-    const int64_t c0 = blk * GPC;
-    const int64_t c1 = min(c0 + (int64_t)GPC, a.n_chunks);
-    const int64_t wlo = a.chunk_root[c0];
-    const int64_t whi = c1 < a.n_chunks ? (int64_t)a.chunk_root[c1] : a.n_roots - 1;
-    const bool priv = whi - wlo + 1 <= CSF_WMAX;
-    if (priv) {
-      for (int i = threadIdx.x; i < (whi - wlo + 1) * G; i += CSF_THREADS) win[i] = zero4;
-      __syncthreads();
-    }
-    const int64_t c = c0 + grp;
-    if (c < c1) {
-      int64_t k = c * a.chunk_nnz;
-      const int64_t kend = min(k + a.chunk_nnz, a.nnz);
-      int64_t s = a.chunk_root[c];
-      int64_t f = a.chunk_fiber[c];
-      int64_t root_end = a.root_ptr[s + 1];
-      // current fiber f and, one ahead, fiber f+1 (its end and factor row)
-      int64_t fib_end = __ldg(a.fib_ptr + f + 1);
-      float4 ua = __ldg(reinterpret_cast<const float4*>(a.Ua + (size_t)__ldg(a.fib_ids + f) * a.R) + sub);
-      int64_t nf_end = fib_end;
-      float4 n_ua = zero4;
-      if (f + 1 < a.n_fibers) {
-        nf_end = __ldg(a.fib_ptr + f + 2);
-        n_ua = __ldg(reinterpret_cast<const float4*>(a.Ua + (size_t)__ldg(a.fib_ids + f + 1) * a.R) + sub);
-      }
-      float4 t = zero4, acc = zero4;
-      while (k < kend) {
-        const int nb = (int)min((int64_t)NB, kend - k);
-        uint32_t b[NB];
-        float v[NB];
+struct BatchMeta {
+  uint32_t off;  // leaf row offset (leaf id * R / 4, float4 units) of entry k + lane
+  float val;
+  uint32_t fend, fid;  // end offset and level-1 id of fiber f + lane
+  uint32_t rend, rid;  // end offset and id of root s + lane
+};
+
+__device__ __forceinline__ BatchMeta load_meta(const Csf3Args& a, uint32_t k, int n, uint32_t f,
+                                               uint32_t s, int lane) {
+  BatchMeta m;
+  const bool e = lane < n;
+  m.off = e ? __ldg(a.leaf_ids + k + lane) * (uint32_t)(a.R / 4) : 0u;
+  m.val = e ? __ldg(a.vals + k + lane) : 0.f;
+  const bool fv = f + lane < (uint32_t)a.n_fibers;
+  m.fend = fv ? __ldg(a.fib_ptr + f + lane + 1) : 0xffffffffu;
+  m.fid = fv ? __ldg(a.fib_ids + f + lane) : 0u;
+  const bool rv = s + lane < (uint32_t)a.n_roots;
+  m.rend = rv ? __ldg(a.root_ptr + s + lane + 1) : 0xffffffffu;
+  m.rid = rv ? __ldg(a.root_ids + s + lane) : 0u;
+  return m;
+}
+
+template <int R>
+struct CsfSlots {
+  static constexpr int LPR = R / 4;           // lanes per factor row (float4 each)
+  static constexpr int SLOTS = 32 / LPR;      // entries per step
+  static constexpr int STEPS = 32 / SLOTS < 8 ? 32 / SLOTS : 8;  // steps per batch
+  static constexpr int BS = SLOTS * STEPS;    // entries per batch (<= 32)
+};
+
+// Sum the per-slot partial root sums of the lanes that share a column quad
+// and add them to output row `rid` (slot-0 lanes issue the atomics).
+template <int R>
+__device__ __forceinline__ void csf_flush(float4& acc, uint32_t rid, int lane, float* M) {
+  constexpr int LPR = CsfSlots<R>::LPR;
 #pragma unroll
-        for (int i = 0; i < NB; ++i) {
-          b[i] = i < nb ? __ldg(a.leaf_ids + k + i) : 0u;
-          v[i] = i < nb ? __ldg(a.vals + k + i) : 0.f;
+  for (int o = LPR; o < 32; o <<= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+    acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+  }
+  if (lane < LPR) atomicAdd(reinterpret_cast<float4*>(M + (size_t)rid * R) + lane, acc);
+  acc = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__device__ __forceinline__ void fma4(float4& acc, float v, const float4& u, const float4& x) {
+  acc.x = fmaf(v * u.x, x.x, acc.x);
+  acc.y = fmaf(v * u.y, x.y, acc.y);
+  acc.z = fmaf(v * u.z, x.z, acc.z);
+  acc.w = fmaf(v * u.w, x.w, acc.w);
+}
+
+template <int R>
+__global__ void __launch_bounds__(CSF_WARPS * 32, 2)
+csf3_slot_kernel(Csf3Args a, int chunks_per_task) {
+  using S = CsfSlots<R>;
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int LPR = S::LPR, SLOTS = S::SLOTS, STEPS = S::STEPS, BS = S::BS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int es = lane / LPR, cq = lane % LPR;  // entry slot, column quad
+  const float4* ub_lane = reinterpret_cast<const float4*>(a.Ub) + cq;
+  const float4* ua_lane = reinterpret_cast<const float4*>(a.Ua) + cq;
+  constexpr uint32_t R4 = R / 4;  // float4 per row
+  const uint32_t nnz = (uint32_t)a.nnz;
+  const uint32_t n_tasks = (uint32_t)((a.n_chunks + chunks_per_task - 1) / chunks_per_task);
+  for (uint32_t task = blockIdx.x * CSF_WARPS + warp; task < n_tasks;
+       task += gridDim.x * CSF_WARPS) {
+    const uint32_t c = task * (uint32_t)chunks_per_task;
+    uint32_t k = c * (uint32_t)a.chunk_nnz;
+    const uint32_t kend = min(k + (uint32_t)(chunks_per_task * a.chunk_nnz), nnz);
+    uint32_t f = a.chunk_fiber[c];
+    uint32_t s = a.chunk_root[c];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t n = min((uint32_t)BS, kend - k);
+    BatchMeta cur = load_meta(a, k, (int)n, f, s, lane);
+    while (k < kend) {
+      // entry k + j ends a fiber / root  <=>  bit j of fmask / rmask
+      const uint32_t fb = (cur.fend > k && cur.fend <= k + n) ? 1u << (cur.fend - k - 1) : 0u;
+      const uint32_t rb = (cur.rend > k && cur.rend <= k + n) ? 1u << (cur.rend - k - 1) : 0u;
+      const uint32_t fmask = __reduce_or_sync(FULL, fb);
+      const uint32_t rmask = __reduce_or_sync(FULL, rb);
+      // entry lane j: its fiber is the number of fiber ends before j; its
+      // fiber row offset (float4 units) comes from that fiber's lane
+      const uint32_t fi_l = __popc(fmask & ((1u << lane) - 1u));
+      const uint32_t fo_l = __shfl_sync(FULL, cur.fid, fi_l) * R4;
+      // leaf rows and fiber rows of the batch, all loads in flight together
+      float4 x[STEPS], u[STEPS];
+      float v[STEPS];
+      if (n == (uint32_t)BS) {
+#pragma unroll
+        for (int st = 0; st < STEPS; ++st) {
+          const int j = st * SLOTS + es;
+          x[st] = __ldg(ub_lane + __shfl_sync(FULL, cur.off, j));
+          u[st] = __ldg(ua_lane + __shfl_sync(FULL, fo_l, j));
+          v[st] = __shfl_sync(FULL, cur.val, j);
         }
-        float4 row[NB];
+      } else {
 #pragma unroll
-        for (int i = 0; i < NB; ++i)
-          row[i] = __ldg(reinterpret_cast<const float4*>(a.Ub + (size_t)b[i] * a.R) + sub);
-#pragma unroll
-        for (int i = 0; i < NB; ++i) {
-          if (i < nb) {
-            t.x = fmaf(v[i], row[i].x, t.x);
-            t.y = fmaf(v[i], row[i].y, t.y);
-            t.z = fmaf(v[i], row[i].z, t.z);
-            t.w = fmaf(v[i], row[i].w, t.w);
-            const int64_t kk = k + i + 1;
-            const bool fiber_done = kk == fib_end;
-            if (fiber_done || kk == kend) {
-              acc.x = fmaf(ua.x, t.x, acc.x);
-              acc.y = fmaf(ua.y, t.y, acc.y);
-              acc.z = fmaf(ua.z, t.z, acc.z);
-              acc.w = fmaf(ua.w, t.w, acc.w);
-              t = zero4;
-              if (fiber_done) {
-                ++f;
-                fib_end = nf_end;
-                ua = n_ua;
-                if (f + 1 < a.n_fibers) {
-                  nf_end = __ldg(a.fib_ptr + f + 2);
-                  n_ua = __ldg(reinterpret_cast<const float4*>(
-                                   a.Ua + (size_t)__ldg(a.fib_ids + f + 1) * a.R) + sub);
-                }
-              }
-              const bool root_done = kk == root_end;
-              if (root_done || kk == kend) {
-                if (priv) {
-                  float* r = reinterpret_cast<float*>(win + (s - wlo) * G + sub);
-                  atomicAdd(r + 0, acc.x);
-                  atomicAdd(r + 1, acc.y);
-                  atomicAdd(r + 2, acc.z);
-                  atomicAdd(r + 3, acc.w);
-                } else {
-                  const uint32_t ri = __ldg(a.root_ids + s);
-                  atomicAdd(reinterpret_cast<float4*>(a.M + (size_t)ri * a.R) + sub, acc);
-                }
-                acc = zero4;
-                if (root_done && ++s < a.n_roots) root_end = __ldg(a.root_ptr + s + 1);
-              }
-            }
+        for (int st = 0; st < STEPS; ++st) {
+          const int j = st * SLOTS + es;
+          const uint32_t xo = __shfl_sync(FULL, cur.off, j);
+          const uint32_t uo = __shfl_sync(FULL, fo_l, j);
+          v[st] = __shfl_sync(FULL, cur.val, j);  // 0 past n
+          x[st] = u[st] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if ((uint32_t)j < n) {
+            x[st] = __ldg(ub_lane + xo);
+            u[st] = __ldg(ua_lane + uo);
           }
         }
-        k += nb;
       }
-    }
-    if (priv) {
-      __syncthreads();
-      for (int i = threadIdx.x; i < (whi - wlo + 1) * G; i += CSF_THREADS) {
-        const int64_t rs = wlo + i / G;
-        const float4 v = win[i];
-        if (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f)
-          atomicAdd(reinterpret_cast<float4*>(a.M + (size_t)a.root_ids[rs] * a.R) + (i % G), v);
+      // next batch's metadata while the rows are in flight
+      const uint32_t kn = k + n;
+      const uint32_t fn = f + __popc(fmask);
+      const uint32_t sn = s + __popc(rmask);
+      const uint32_t nn = min((uint32_t)BS, kend - kn);
+      BatchMeta nxt = cur;
+      if (kn < kend) nxt = load_meta(a, kn, (int)nn, fn, sn, lane);
+      int ri = 0;
+      if (rmask == 0u) {
+#pragma unroll
+        for (int st = 0; st < STEPS; ++st) fma4(acc, v[st], u[st], x[st]);
+      } else {
+        // root ends inside the batch: add and flush segment by segment
+#pragma unroll
+        for (int st = 0; st < STEPS; ++st) {
+          uint32_t rs = (rmask >> (st * SLOTS)) & ((SLOTS < 32 ? (1u << SLOTS) : 0u) - 1u);
+          int lo = 0;
+          while (rs) {
+            const int e = __ffs(rs) - 1;
+            rs &= rs - 1u;
+            if (es >= lo && es <= e) fma4(acc, v[st], u[st], x[st]);
+            csf_flush<R>(acc, __shfl_sync(FULL, cur.rid, ri), lane, a.M);
+            ++ri;
+            lo = e + 1;
+          }
+          if (es >= lo) fma4(acc, v[st], u[st], x[st]);
+        }
       }
-      __syncthreads();
+      // task end: the open root's sum
+      if (kn == kend && !((rmask >> (n - 1)) & 1u))
+        csf_flush<R>(acc, __shfl_sync(FULL, cur.rid, ri), lane, a.M);
+      k = kn;
+      f = fn;
+      s = sn;
+      n = nn;
+      cur = nxt;
     }
   }
 }
@@ -544,16 +596,20 @@ __global__ void csf_generic_mttkrp_kernel(CsfGenArgs a) {
   }
 }
 
-template <int G>
-void launch_csf3(tsr_ctx* ctx, cudaStream_t s, const Csf3Args& a) {
-  const int64_t gpc = CSF_THREADS / G;
-  const int64_t blocks = ceil_div(a.n_chunks, gpc);
-  const int64_t cap = (int64_t)std::max(1, ctx->sm_count - ctx->reserve_sms) * 4;
+template <int R>
+void launch_csf3_slot(tsr_ctx* ctx, cudaStream_t s, const Csf3Args& a) {
+  constexpr int kChunksPerTask = 4;  // 1024 entries per warp task
+  const int64_t tasks = ceil_div(a.n_chunks, kChunksPerTask);
+  const int64_t blocks = ceil_div(tasks, CSF_WARPS);
+  const int64_t cap = (int64_t)std::max(1, ctx->sm_count - ctx->reserve_sms) * 2;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min(blocks, cap));
-  csf3_mttkrp_kernel<G><<<grid, CSF_THREADS, sizeof(float4) * CSF_WMAX * G, s>>>(a);
+  csf3_slot_kernel<R><<<grid, CSF_WARPS * 32, 0, s>>>(a, kChunksPerTask);
 }
 
+
 }  // namespace
+
+void init_csf_attributes() {}  // the CSF kernels use no dynamic shared memory
 
 int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const FactorTable& ft,
                       int R, int mode, float* d_out) {
@@ -581,16 +637,19 @@ int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const 
     a.Ub = ft.ptr[c.mode_order[2]];
     a.R = R;
     a.M = d_out;
-    switch (R / 4) {
-      case 1: launch_csf3<1>(ctx, s, a); break;
-      case 2: launch_csf3<2>(ctx, s, a); break;
-      case 4: launch_csf3<4>(ctx, s, a); break;
-      case 8: launch_csf3<8>(ctx, s, a); break;
-      case 16: launch_csf3<16>(ctx, s, a); break;
-      case 32: launch_csf3<32>(ctx, s, a); break;
-      default: vec = false;
-    }
-    if (vec) {
+    // rows of a factor are addressed with 32-bit element offsets
+    bool fast = R == 4 || R == 8 || R == 16 || R == 32 || R == 64 || R == 128;
+    for (int l = 1; l < 3 && fast; ++l)
+      fast = (uint64_t)sp->shape[c.mode_order[l]] * (uint64_t)R < 0xffffffffull;
+    if (fast) {
+      switch (R) {
+        case 4: launch_csf3_slot<4>(ctx, s, a); break;
+        case 8: launch_csf3_slot<8>(ctx, s, a); break;
+        case 16: launch_csf3_slot<16>(ctx, s, a); break;
+        case 32: launch_csf3_slot<32>(ctx, s, a); break;
+        case 64: launch_csf3_slot<64>(ctx, s, a); break;
+        default: launch_csf3_slot<128>(ctx, s, a); break;
+      }
       ctx->launches++;
       TSR_CUDA(cudaGetLastError());
       return TSR_OK;

@@ -43,5 +43,7 @@ namespace tsr {
 // here). Factors are device pointers (row-major I_m x R).
 int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const FactorTable& ft,
                       int R, int mode, float* d_out);
+// Shared-memory limits of the CSF kernels (once per process, before capture).
+void init_csf_attributes();
 
 }  // namespace tsr

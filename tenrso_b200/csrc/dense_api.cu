@@ -11,11 +11,10 @@
 
 #include "als.cuh"
 #include "csf.cuh"
-#include "mttkrp.cuh"
+#include "dense.cuh"
 
 namespace tsr {
 
-namespace {
 
 // mttkrp.rs:86-122 then the KR helper's bail (mttkrp.rs:196-198).
 int validate_mttkrp(int ndim, const int64_t* shape, int n_factors, const int64_t* frows,
@@ -47,7 +46,7 @@ int64_t numel(int ndim, const int64_t* shape) {
   return n;
 }
 
-bool is_row_major(int ndim, const int64_t* shape, const int64_t* strides) {
+static bool is_row_major(int ndim, const int64_t* shape, const int64_t* strides) {
   if (!strides) return true;
   int64_t s = 1;
   for (int d = ndim - 1; d >= 0; --d) {
@@ -58,7 +57,7 @@ bool is_row_major(int ndim, const int64_t* shape, const int64_t* strides) {
 }
 
 // ndarray's as_standard_layout (mttkrp.rs:172-173): pack a strided host view.
-void pack_host(const float* src, int ndim, const int64_t* shape, const int64_t* strides,
+static void pack_host(const float* src, int ndim, const int64_t* shape, const int64_t* strides,
                float* dst) {
   int64_t n = numel(ndim, shape);
   std::vector<int64_t> idx(ndim, 0);
@@ -92,25 +91,57 @@ int upload_tensor(tsr_ctx* ctx, const float* host, int ndim, const int64_t* shap
   return TSR_OK;
 }
 
-// Per-mode operand of the MTTKRP: unfolding copies in the precision needed.
-struct ModeOperand {
-  Unfolding u;
-  const float* f32 = nullptr;
-  const __nv_bfloat16* hi = nullptr;
-  const __nv_bfloat16* lo = nullptr;
-};
+int upload_factors(tsr_ctx* ctx, int ndim, const int64_t* shape, const float* const* factors,
+                   int64_t R, FactorTable* ft) {
+  int64_t total = 0;
+  for (int m = 0; m < ndim; ++m) total += shape[m] * R;
+  void* d;
+  TSR_TRY(slot_get(ctx, SLOT_FACTORS, sizeof(float) * total, &d));
+  float* p = (float*)d;
+  for (int m = 0; m < ndim; ++m) {
+    TSR_CUDA(cudaMemcpyAsync(p, factors[m], sizeof(float) * shape[m] * R, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    ft->ptr[m] = p;
+    ft->rows[m] = shape[m];
+    p += shape[m] * R;
+  }
+  return TSR_OK;
+}
 
-int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int mode,
-                 int precision, int slot_index, ModeOperand* op) {
+// SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform.
+static uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
+  const uint64_t golden = 0x9E3779B97F4A7C15ull;
+  uint64_t key = mix64(seed * 0x100000001B3ull + stream * 0x2545F4914F6CDD1Dull + golden);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t r = mix64(key + (uint64_t)i * golden);
+    out[i] = (float)((double)(r >> 11) * (1.0 / 9007199254740992.0));
+  }
+}
+
+// Per-mode operand of the MTTKRP: unfolding copies in the precision needed.
+void mode_operand_bytes(const Unfolding& u, int precision, size_t* a_bytes, size_t* b_bytes) {
+  if (precision == TSR_PREC_BF16X3) {
+    *a_bytes = *b_bytes = 2 * (size_t)u.rows * u.ld;
+  } else {
+    *a_bytes = (u.mode == 0 && u.ld == u.cols) ? 0 : sizeof(float) * (size_t)u.rows * u.ld;
+    *b_bytes = 0;
+  }
+}
+
+int prepare_mode_into(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int mode,
+                      int precision, void* buf_a, void* buf_b, ModeOperand* op) {
   op->u = make_unfolding(ndim, shape, mode);
   const Unfolding& u = op->u;
   if (precision == TSR_PREC_BF16X3) {
-    void *hi, *lo;
-    TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + slot_index, 2 * u.rows * u.ld, &hi));
-    TSR_TRY(slot_get(ctx, SLOT_UNFOLD_LO + slot_index, 2 * u.rows * u.ld, &lo));
-    TSR_TRY(launch_unfold_bf16x2(ctx, dX, shape, u, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo));
-    op->hi = (const __nv_bfloat16*)hi;
-    op->lo = (const __nv_bfloat16*)lo;
+    TSR_TRY(launch_unfold_bf16x2(ctx, dX, shape, u, (__nv_bfloat16*)buf_a,
+                                 (__nv_bfloat16*)buf_b));
+    op->hi = (const __nv_bfloat16*)buf_a;
+    op->lo = (const __nv_bfloat16*)buf_b;
     return TSR_OK;
   }
   // mode 0 of a row-major tensor is already its unfolding when rows are aligned
@@ -118,11 +149,19 @@ int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, 
     op->f32 = dX;
     return TSR_OK;
   }
-  void* p;
-  TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + slot_index, sizeof(float) * u.rows * u.ld, &p));
-  TSR_TRY(launch_unfold_f32(ctx, dX, shape, u, (float*)p));
-  op->f32 = (const float*)p;
+  TSR_TRY(launch_unfold_f32(ctx, dX, shape, u, (float*)buf_a));
+  op->f32 = (const float*)buf_a;
   return TSR_OK;
+}
+
+int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int mode,
+                 int precision, int slot_index, ModeOperand* op) {
+  size_t ab, bb;
+  mode_operand_bytes(make_unfolding(ndim, shape, mode), precision, &ab, &bb);
+  void *a = nullptr, *b = nullptr;
+  if (ab) TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + slot_index, ab, &a));
+  if (bb) TSR_TRY(slot_get(ctx, SLOT_UNFOLD_LO + slot_index, bb, &b));
+  return prepare_mode_into(ctx, dX, ndim, shape, mode, precision, a, b, op);
 }
 
 // Split-K partial MTTKRP of one mode into `partials` (allocated here).
@@ -162,40 +201,6 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
   TSR_TRY(launch_mttkrp_reduce(ctx, partials, splits, op.u.rows * R, d_out));
   return TSR_OK;
 }
-
-int upload_factors(tsr_ctx* ctx, int ndim, const int64_t* shape, const float* const* factors,
-                   int64_t R, FactorTable* ft) {
-  int64_t total = 0;
-  for (int m = 0; m < ndim; ++m) total += shape[m] * R;
-  void* d;
-  TSR_TRY(slot_get(ctx, SLOT_FACTORS, sizeof(float) * total, &d));
-  float* p = (float*)d;
-  for (int m = 0; m < ndim; ++m) {
-    TSR_CUDA(cudaMemcpyAsync(p, factors[m], sizeof(float) * shape[m] * R, cudaMemcpyHostToDevice,
-                             ctx->stream));
-    ft->ptr[m] = p;
-    ft->rows[m] = shape[m];
-    p += shape[m] * R;
-  }
-  return TSR_OK;
-}
-
-// SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform.
-uint64_t mix64(uint64_t z) {
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
-  const uint64_t golden = 0x9E3779B97F4A7C15ull;
-  uint64_t key = mix64(seed * 0x100000001B3ull + stream * 0x2545F4914F6CDD1Dull + golden);
-  for (int64_t i = 0; i < n; ++i) {
-    uint64_t r = mix64(key + (uint64_t)i * golden);
-    out[i] = (float)((double)(r >> 11) * (1.0 / 9007199254740992.0));
-  }
-}
-
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // CP-ALS driver (cp/core.rs:91-214) on a device-resident tensor.
@@ -336,7 +341,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     TSR_CUDA(cudaMemcpyAsync(&a.b.state->xnorm_sq, &sp->norm_sq, sizeof(double),
                              cudaMemcpyHostToDevice, ctx->stream));
   else
-    TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, a.b.state));
+    TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, &a.b.state->xnorm_sq));
   for (int m = 0; m < ndim; ++m)
     TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
                         a.b.grams + (size_t)m * R * R, false));
@@ -416,6 +421,8 @@ void init_kernel_attributes() {
   init_tc_attributes();
   init_simt_attributes();
   init_als_attributes();
+  init_adjoint_attributes();
+  init_csf_attributes();
   done = true;
 }
 

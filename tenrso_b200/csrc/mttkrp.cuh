@@ -17,6 +17,9 @@ SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
 int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
                        const SplitPlan& plan, float* partials);
 int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out);
+// Same for a rows x R result, each column r scaled by w[r] when w is given.
+int launch_mttkrp_reduce_scaled(tsr_ctx* ctx, const float* partials, int splits, int64_t rows,
+                                int R, const float* w, float* out);
 
 // BF16x3 tcgen05 kernel (mttkrp_tc.cu). The unfolding halves hi/lo are bf16
 // with row stride u.ld (a multiple of 8 elements, 16 bytes).

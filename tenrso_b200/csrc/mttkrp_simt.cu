@@ -153,14 +153,37 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
   }
 }
 
-__global__ void mttkrp_reduce_kernel(const float* __restrict__ partials, int splits, int64_t n,
-                                     float* __restrict__ out) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+// out[e] = sum over splits of partials[s][e] (FP64), optionally times w[e % R].
+// `groups` threads share an element, each summing every groups-th split with
+// four loads in flight; the groups combine through shared memory.
+__global__ void __launch_bounds__(256)
+mttkrp_reduce_kernel(const float* __restrict__ partials, int splits, int64_t n, int groups,
+                     int R, const float* __restrict__ w, float* __restrict__ out) {
+  __shared__ double red[256];
+  const int per = 256 / groups;
+  const int g = threadIdx.x / per, l = threadIdx.x % per;
+  const int64_t k = (int64_t)blockIdx.x * per + l;
   double s = 0.0;
-  for (int p = 0; p < splits; ++p) s += (double)__ldg(partials + (int64_t)p * n + k);
+  if (k < n) {
+    const float* p = partials + k;
+    int q = g;
+    for (; q + 3 * groups < splits; q += 4 * groups) {
+      const float v0 = __ldg(p + (int64_t)q * n);
+      const float v1 = __ldg(p + (int64_t)(q + groups) * n);
+      const float v2 = __ldg(p + (int64_t)(q + 2 * groups) * n);
+      const float v3 = __ldg(p + (int64_t)(q + 3 * groups) * n);
+      s += ((double)v0 + (double)v1) + ((double)v2 + (double)v3);
+    }
+    for (; q < splits; q += groups) s += (double)__ldg(p + (int64_t)q * n);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  if (g != 0 || k >= n) return;
+  for (int j = 1; j < groups; ++j) s += red[j * per + l];
+  if (w) s *= (double)__ldg(w + (int)(k % R));
   out[k] = (float)s;
 }
+
 // khatri_rao.rs:56-89: C[a*J + b, k] = A[a, k] * B[b, k].
 __global__ void khatri_rao_kernel(const float* __restrict__ A, int64_t I,
                                   const float* __restrict__ B, int64_t J, int64_t K,
@@ -216,12 +239,22 @@ int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const K
   return TSR_OK;
 }
 
-int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out) {
-  mttkrp_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, ctx->stream>>>(partials, splits, n,
-                                                                            out);
+int launch_mttkrp_reduce_scaled(tsr_ctx* ctx, const float* partials, int splits, int64_t rows,
+                                int R, const float* w, float* out) {
+  const int64_t n = rows * R;
+  if (n == 0) return TSR_OK;
+  int groups = 1;
+  while (groups < 8 && 2 * groups <= splits) groups *= 2;
+  const int per = 256 / groups;
+  mttkrp_reduce_kernel<<<(unsigned)ceil_div(n, per), 256, 0, ctx->stream>>>(
+      partials, splits, n, groups, R > 0 ? R : 1, w, out);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
+}
+
+int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out) {
+  return launch_mttkrp_reduce_scaled(ctx, partials, splits, n, 1, nullptr, out);
 }
 
 }  // namespace tsr

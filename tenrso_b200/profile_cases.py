@@ -84,6 +84,10 @@ def case_csf_mttkrp(args):
     torch.cuda.synchronize()
     print("csf_mttkrp", shape, "nnz", n, "rank", args.rank, "mode", args.mode,
           "checksum", float(M.double().sum()), sp.info(args.mode))
+    if args.time:
+        ms = sp.profile_mttkrp_dev([f.data_ptr() for f in fs], args.rank, args.mode, iters=10,
+                                   flush_l2=True)
+        print(f"csf_mttkrp kernel {ms:.4f} ms (L2 flushed, mean of 10)")
     sp.close()
 
 
@@ -101,6 +105,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--launches", type=int, default=1)
     ap.add_argument("--nnz", type=int, default=20_000_000)
+    ap.add_argument("--time", action="store_true", help="also print the kernel time")
     args = ap.parse_args(argv)
     CASES[args.case](args)
 

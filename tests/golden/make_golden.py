@@ -29,6 +29,39 @@ def manual_mttkrp_mode1():
     return out.tolist()
 
 
+def cp_grad_definition(factors, shape, weights=None):
+    # dL/dU_n[i, r] = w_r * sum over the other indices of G * prod_{m != n} U_m[i_m, r]
+    # with G = ones (crates/tenrso-ad/src/grad.rs:81-120 applied to DenseND::ones)
+    U = [np.array(f, dtype=np.float64) for f in factors]
+    R = U[0].shape[1]
+    w = np.ones(R) if weights is None else np.array(weights, dtype=np.float64)
+    out = []
+    for n in range(len(U)):
+        g = np.zeros((shape[n], R))
+        for r in range(R):
+            p = w[r]
+            for m in range(len(U)):
+                if m != n:
+                    p *= U[m][:, r].sum()
+            g[:, r] = p
+        out.append(g.tolist())
+    return out
+
+
+def reconstruct_definition(factors, weights=None):
+    # crates/tenrso-kernels/src/outer.rs:223-274 for two factors: A diag(w) B^T
+    A, B = (np.array(f, dtype=np.float64) for f in factors)
+    w = np.ones(A.shape[1]) if weights is None else np.array(weights, dtype=np.float64)
+    return ((A * w) @ B.T).tolist()
+
+
+GRAD_FACTORS_3WAY = [
+    np.arange(1, 13, dtype=np.float64).reshape(4, 3).tolist(),
+    (np.arange(1, 16, dtype=np.float64) / 10).reshape(5, 3).tolist(),
+    [[1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0.5, 0], [0, 0.5, 0.5], [0.5, 0, 0.5]],
+]
+GRAD_FACTORS_W = [[[1, 2], [3, 4], [5, 6]], [[0.1, 0.2], [0.3, 0.4], [0.5, 0.6], [0.7, 0.8]]]
+
 KATS = {
     "khatri_rao": [
         {"src": "crates/tenrso-kernels/src/khatri_rao.rs:41-55,479-498",
@@ -93,6 +126,34 @@ KATS = {
         {"src": "crates/tenrso-sparse/src/csf.rs:637-648", "shape": [5, 5, 5],
          "indices": [[2, 3, 4]], "values": [42], "mode_order": [0, 1, 2],
          "fptr": [[0, 1], [0, 1], [0, 1]], "fids": [[2], [3], [4]], "vals": [42]},
+    ],
+    "cp_reconstruct": [
+        {"src": "crates/tenrso-kernels/src/outer.rs:440-455", "factors": [[[2], [3]], [[4], [5], [6]]],
+         "weights": None, "shape": [2, 3], "expected": [[8, 10, 12], [12, 15, 18]]},
+        {"src": "crates/tenrso-kernels/src/outer.rs:457-470",
+         "factors": [[[1, 0], [0, 1]], [[1, 0], [0, 1]]], "weights": None, "shape": [2, 2],
+         "expected": [[1, 0], [0, 1]]},
+        {"src": "crates/tenrso-kernels/src/outer.rs:473-483 (pins [0,0] = 46; the rest is "
+                "the definition)", "factors": [[[1, 2], [3, 4]], [[5, 6], [7, 8]]],
+         "weights": [2, 3], "shape": [2, 2],
+         "expected": reconstruct_definition([[[1, 2], [3, 4]], [[5, 6], [7, 8]]], [2, 3])},
+        {"src": "crates/tenrso-kernels/src/outer.rs:213-222 (doc example, shape only; values "
+                "are the definition)",
+         "factors": [[[1, 0], [0, 1]], [[1, 0], [0, 1], [1, 1]]], "weights": None,
+         "shape": [2, 3],
+         "expected": reconstruct_definition([[[1, 0], [0, 1]], [[1, 0], [0, 1], [1, 1]]])},
+    ],
+    "cp_reconstruct_errors": [
+        {"src": "crates/tenrso-kernels/src/outer.rs:512-520",
+         "factors": [[[1, 2], [3, 4]], [[5], [6]]], "expect": "columns"},
+    ],
+    "cp_grad": [
+        {"src": "crates/tenrso-ad/tests/integration_tests.rs:56-99 (ones gradient)",
+         "factors": GRAD_FACTORS_3WAY, "weights": None, "shape": [4, 5, 6],
+         "expected": cp_grad_definition(GRAD_FACTORS_3WAY, [4, 5, 6])},
+        {"src": "crates/tenrso-ad/tests/integration_tests.rs:335-367 (weights)",
+         "factors": GRAD_FACTORS_W, "weights": [2, 3], "shape": [3, 4],
+         "expected": cp_grad_definition(GRAD_FACTORS_W, [3, 4], [2, 3])},
     ],
     "csf_errors": [
         {"src": "crates/tenrso-sparse/src/csf.rs:516-531", "ndim": 3,

@@ -93,3 +93,26 @@ def test_no_cpu_fallback_without_device():
     rc = lib.tsr_ctx_create(0, None, C.byref(h))
     assert rc == 9  # TSR_E_CUDA
     assert lib.tsr_last_error()
+
+
+def test_cp_reconstruct_errors(kats):
+    k = kats["cp_reconstruct_errors"][0]
+    with pytest.raises(tb.TenrsoError, match=k["expect"]):
+        tb.cp_reconstruct([np.array(f, np.float32) for f in k["factors"]])
+    with pytest.raises(tb.TenrsoError, match="Factor 1 has 1 columns, expected 2"):
+        tb.cp_reconstruct([np.array(f, np.float32) for f in k["factors"]])
+    with pytest.raises(tb.TenrsoError,
+                       match="Need at least one factor matrix for CP reconstruction"):
+        tb.cp_reconstruct([])
+    with pytest.raises(tb.TenrsoError, match="Weights length 3 must match rank 2"):
+        tb.cp_reconstruct([np.ones((2, 2), np.float32)] * 2, weights=[1, 2, 3])
+
+
+def test_cp_reconstruction_grad_errors():
+    fs = [np.ones((n, 2), np.float32) for n in (3, 4, 5)]
+    g = tb.CpReconstructionGrad(fs)
+    with pytest.raises(tb.TenrsoError, match="Gradient rank 2 doesn't match number of factors 3"):
+        g.compute_factor_gradients(np.ones((3, 4), np.float32))
+    one = tb.CpReconstructionGrad([np.ones((3, 2), np.float32)])
+    with pytest.raises(tb.TenrsoError, match="Need at least one factor for Khatri-Rao product"):
+        one.compute_factor_gradients(np.ones((3,), np.float32))

@@ -149,3 +149,38 @@ def test_coo_mttkrp_matches_dense(orc):
     for mode in range(3):
         assert np.allclose(orc.coo_mttkrp(idx, vals, shape, fs, mode),
                            orc.mttkrp(X, fs, mode), rtol=1e-12, atol=1e-12)
+
+
+def test_cp_reconstruct_golden(orc, kats):
+    for case in kats["cp_reconstruct"]:
+        fs = [np.array(f, float) for f in case["factors"]]
+        Xh = orc.cp_reconstruct(fs, case["weights"])
+        assert list(Xh.shape) == case["shape"], case["src"]
+        assert np.array_equal(Xh, np.array(case["expected"], float)), case["src"]
+
+
+def test_cp_grad_golden(orc, kats):
+    for case in kats["cp_grad"]:
+        fs = [np.array(f, float) for f in case["factors"]]
+        G = np.ones(case["shape"])
+        gs = orc.cp_reconstruction_grad(fs, G, case["weights"])
+        for g, f, e in zip(gs, fs, case["expected"]):
+            assert g.shape == f.shape, case["src"]
+            assert np.allclose(g, np.array(e), rtol=1e-12, atol=0), case["src"]
+            assert abs(g.sum()) > 1e-6  # the reference's own assertion
+
+
+@pytest.mark.parametrize("shape,R", [((6, 5, 4, 3), 3), ((7, 4), 2), ((5, 4, 3), 4)])
+def test_cp_vjp_vs_central_differences(orc, shape, R):
+    """The CPU VJP (restated reconstruction + CpReconstructionGrad on
+    G = 2(Xhat - X), plus 2 reg U) equals FP64 central differences (h=1e-6)
+    of ||X - [[U]]||^2 + reg sum ||U||^2 in every factor entry."""
+    rng = np.random.default_rng(R)
+    X = rng.standard_normal(shape)
+    fs = [rng.standard_normal((n, R)) for n in shape]
+    _, g = orc.cp_loss_grad_vjp(X, fs, 1e-3)
+    for m in range(len(shape)):
+        ent = [(i, r) for i in range(shape[m]) for r in range(R)]
+        fd = orc.fd_grad_entries(X, fs, 1e-3, m, ent)
+        an = np.array([g[m][i, r] for i, r in ent])
+        assert np.abs(fd - an).max() <= 1e-7 * np.abs(an).max(), m

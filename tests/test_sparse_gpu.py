@@ -99,7 +99,7 @@ def test_csf_empty_and_errors():
             tb.CsfTensor.from_coo(coo, bad)
 
 
-@pytest.mark.parametrize("R", [32, 8, 4, 64, 5])
+@pytest.mark.parametrize("R", [32, 8, 4, 64, 5, 128, 96])
 @pytest.mark.parametrize("shape", [(60, 50, 40), (300, 7, 90)])
 def test_csf_mttkrp_parity(orc, shape, R):
     idx, vals = random_coo(shape, 20000, seed=R, dup_frac=0.2)
@@ -174,3 +174,62 @@ def test_device_zipf_generator_matches_numpy():
     coo.deduplicate()
     assert np.array_equal(d_idx[:m * 3].cpu().numpy().reshape(m, 3), coo.indices())
     assert np.array_equal(d_val[:m].cpu().numpy(), coo.values())
+
+
+def _zipf_device_coo(shape, nnz, seed):
+    """Device-drawn Zipf(1.2) COO, merged; returns (SparseTensor, host idx, host vals)."""
+    import torch
+    cap = 12 * nnz
+    d_idx = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_val = torch.empty(cap, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    n_raw = tb.synth_zipf_coo_dev(shape, nnz, seed, d_idx.data_ptr(), d_val.data_ptr(), cap)
+    n = tb.coo_deduplicate_dev(d_idx.data_ptr(), d_val.data_ptr(), n_raw, shape)
+    sp = tb.SparseTensor(d_indices=d_idx.data_ptr(), d_values=d_val.data_ptr(), nnz=n,
+                         shape=shape)
+    torch.cuda.synchronize()
+    idx = d_idx[:3 * n].view(n, 3).cpu().numpy()
+    vals = d_val[:n].cpu().numpy()
+    return sp, idx, vals
+
+
+def test_csf_mttkrp_at_scale(orc):
+    """8e6 merged Zipf entries: every warp of the CSF kernel walks several
+    tasks and heavy roots span many tasks."""
+    shape = (40000, 32000, 4000)
+    sp, idx, vals = _zipf_device_coo(shape, 8_000_000, 0xC3)
+    rng = np.random.default_rng(3)
+    for R in (32, 64):
+        fs = [rng.random((n, R)).astype(np.float32) for n in shape]
+        for mode in range(3):
+            out = sp.mttkrp(fs, mode)
+            ref = orc.coo_mttkrp(idx, vals.astype(np.float64), shape,
+                                 [f.astype(np.float64) for f in fs], mode)
+            assert rel_err(out, ref) <= 1e-5, (R, mode, rel_err(out, ref))
+    sp.close()
+
+
+def test_sparse_cp_als_fit_at_scale():
+    """Sparse CP-ALS fit at 2e6 entries against an independent FP64 fit of the
+    returned factors: ||X - Xhat||^2 = ||X||^2 - 2 sum_nz v Xhat + sum prod Grams."""
+    shape = (20000, 16000, 2000)
+    sp, idx, vals = _zipf_device_coo(shape, 2_000_000, 0xC4)
+    R = 16
+    init = synth.init_factors(shape, R, 0xC4)
+    res = sp.cp_als(R, 6, 0.0, init=init)
+    U = [f.astype(np.float64) for f in res.factors]
+    v = vals.astype(np.float64)
+    inner = 0.0
+    for a in range(0, len(v), 500_000):
+        sl = slice(a, a + 500_000)
+        p = U[0][idx[sl, 0]] * U[1][idx[sl, 1]] * U[2][idx[sl, 2]]
+        inner += float(v[sl] @ p.sum(axis=1))
+    G = np.ones((R, R))
+    for f in U:
+        G *= f.T @ f
+    xn = float(v @ v)
+    fit = 1.0 - np.sqrt(max(xn - 2 * inner + G.sum(), 0.0)) / np.sqrt(xn)
+    assert res.iters == 6
+    assert abs(res.fit - fit) <= 1e-4, (res.fit, fit)
+    assert res.fit < 1.0
+    sp.close()
