@@ -268,6 +268,42 @@ int tsr_dense_destroy(tsr_dense* X);
 int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* const* d_factors,
                              int64_t rank, double reg, float* const* d_grads, double* loss);
 
+/* ---- batched CP-ALS (no tenrso counterpart; each instance is cp_als,
+ * crates/tenrso-decomp/src/cp/core.rs:91-214, from injected factors) -------
+ * A device-resident batch of n_inst dense 3-way tensors: shapes is n_inst x 3,
+ * ranks n_inst (1 <= rank <= min(shape), rank <= 16), tensors[b] a host
+ * row-major fp32 tensor. Factors of the whole batch are one packed array:
+ * instance b at offsets[b] (tsr_batch_factor_layout) holds A | B | C, each
+ * row-major with row stride rank. All instances run in one persistent
+ * launch per run (a CUDA graph captured on first use and replayed). */
+typedef struct tsr_batch tsr_batch;
+int tsr_batch_create_f32(tsr_ctx* ctx, int n_inst, const int64_t* shapes, const int64_t* ranks,
+                         const float* const* tensors, tsr_batch** out);
+int tsr_batch_destroy(tsr_batch* batch);
+int tsr_batch_factor_layout(const tsr_batch* batch, int64_t* total_floats, int64_t* offsets);
+/* Launch configuration: threads per instance CTA (128, 256 or 512), sweeps
+ * per launch (0 = all iterations in one launch), resident CTAs per SM (1-4).
+ * tsr_batch_autotune chooses it by timing; set/get override or read it. */
+int tsr_batch_set_config(tsr_batch* batch, int threads, int sweeps_per_launch, int ctas_per_sm);
+int tsr_batch_get_config(const tsr_batch* batch, int* threads, int* sweeps_per_launch,
+                         int* ctas_per_sm);
+/* Times the candidate configurations on this batch (max_iters sweeps each,
+ * from d_init) and keeps the fastest; the result is cached in the JSON file
+ * cache_path (NULL = no cache) under the device name and the batch's shape
+ * signature, and read back from there on later calls. */
+int tsr_batch_autotune(tsr_ctx* ctx, tsr_batch* batch, int max_iters, const float* d_init,
+                       const char* cache_path, int* from_cache);
+/* cp_als on every instance: max_iters, tol as cp_als; init = packed initial
+ * factors (host; NULL = U(0,1) from the seeded stream seed + instance);
+ * out = packed factors (host); infos = n_inst results (fit_history pointers
+ * may be NULL). */
+int tsr_cp_als_batched_f32(tsr_ctx* ctx, tsr_batch* batch, int max_iters, double tol,
+                           const float* init, uint64_t seed, float* out, tsr_cp_info* infos);
+/* Device-resident form: d_init / d_out packed device arrays (may alias);
+ * infos may be NULL (then the call does not synchronize). */
+int tsr_cp_als_batched_dev_f32(tsr_ctx* ctx, tsr_batch* batch, int max_iters, double tol,
+                               const float* d_init, float* d_out, tsr_cp_info* infos);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,4 +44,6 @@ from .adjoint import (  # noqa: F401
     reconstruction_grad_dev,
 )
 
+from .batched import BatchedCpAls  # noqa: F401
+
 __version__ = "0.1.0"

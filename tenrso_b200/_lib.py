@@ -81,6 +81,15 @@ SIGNATURES = {
     "tsr_dense_create_dev_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(P)]),
     "tsr_dense_destroy": (C.c_int, [P]),
     "tsr_cp_loss_grad_dev_f32": (C.c_int, [P, P, P, I64, C.c_double, P, C.POINTER(C.c_double)]),
+    "tsr_batch_create_f32": (C.c_int, [P, C.c_int, P, P, P, C.POINTER(P)]),
+    "tsr_batch_destroy": (C.c_int, [P]),
+    "tsr_batch_factor_layout": (C.c_int, [P, PI64, P]),
+    "tsr_batch_set_config": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
+    "tsr_batch_get_config": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int)]),
+    "tsr_batch_autotune": (C.c_int, [P, P, C.c_int, P, C.c_char_p, C.POINTER(C.c_int)]),
+    "tsr_cp_als_batched_f32": (C.c_int, [P, P, C.c_int, C.c_double, P, C.c_uint64, P, P]),
+    "tsr_cp_als_batched_dev_f32": (C.c_int, [P, P, C.c_int, C.c_double, P, P, P]),
 }
 
 _lib = None

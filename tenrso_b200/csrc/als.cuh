@@ -30,6 +30,36 @@ struct AlsBuffers {
   double* history;  // [max_iters]
 };
 
+// 16 x 16 Gauss-Jordan inverse held by one warp: lane owns P[r][c] for
+// r = (lane >> 4) + 2q (q < 8), c = lane & 15. Pivot rows/columns move by
+// shuffles; returns false on a pivot that is not positive or not finite.
+__device__ __forceinline__ bool warp_gj16(double (&v)[8], int lane) {
+  const int c = lane & 15, r0 = lane >> 4;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int krow_lane = (k & 1) * 16;  // lanes holding row k
+    const double p = __shfl_sync(0xffffffffu, v[k >> 1], krow_lane + k);
+    const double pkc = __shfl_sync(0xffffffffu, v[k >> 1], krow_lane + c);
+    double prk[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) prk[q] = __shfl_sync(0xffffffffu, v[q], r0 * 16 + k);
+    ok = ok && (p > 0.0) && isfinite(p);
+    const double inv = __drcp_rn(p);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int r = r0 + 2 * q;
+      if (r == k)
+        v[q] = (c == k) ? inv : v[q] * inv;
+      else if (c == k)
+        v[q] = -prk[q] * inv;
+      else
+        v[q] = v[q] - prk[q] * (pkc * inv);
+    }
+  }
+  return ok;
+}
+
 void init_als_attributes();
 // Upper triangle of U^T U (FP64) accumulated into gram; zero_first memsets it.
 int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int R,

@@ -47,5 +47,10 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
 int launch_reconstruct(tsr_ctx* ctx, const FactorTable& ft, int ndim, int R, const float* w,
                        const float* X, float alpha, double* sq_err, float* out);
 void init_adjoint_attributes();
+void init_batched_attributes();
+
+// SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform (the
+// library's InitStrategy::Random).
+void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out);
 
 }  // namespace tsr

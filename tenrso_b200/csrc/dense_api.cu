@@ -109,12 +109,12 @@ int upload_factors(tsr_ctx* ctx, int ndim, const int64_t* shape, const float* co
 }
 
 // SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform.
-static uint64_t mix64(uint64_t z) {
+uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
-static void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
+void seeded_uniform(uint64_t seed, uint64_t stream, int64_t n, float* out) {
   const uint64_t golden = 0x9E3779B97F4A7C15ull;
   uint64_t key = mix64(seed * 0x100000001B3ull + stream * 0x2545F4914F6CDD1Dull + golden);
   for (int64_t i = 0; i < n; ++i) {
@@ -423,6 +423,7 @@ void init_kernel_attributes() {
   init_als_attributes();
   init_adjoint_attributes();
   init_csf_attributes();
+  init_batched_attributes();
   done = true;
 }
 

@@ -91,7 +91,52 @@ def case_csf_mttkrp(args):
     sp.close()
 
 
-CASES = {"mttkrp": case_mttkrp, "cp_als": case_cp_als, "csf_mttkrp": case_csf_mttkrp}
+def case_loss_grad(args):
+    """Gram-form loss/gradient of ||X - [[A,B,C,D]]||^2 + 1e-3 sum ||U||^2 at
+    128x96x64x48, rank 32 (seeded N(0,1))."""
+    import torch
+
+    import tenrso_b200 as tb
+    ctx = _ctx()
+    shape = (128, 96, 64, 48)
+    rng = np.random.default_rng(0xC5)
+    X = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    fs = [torch.from_numpy(rng.standard_normal((n, args.rank)).astype(np.float32)).cuda()
+          for n in shape]
+    gs = [torch.empty_like(f) for f in fs]
+    d = tb.DenseTensor(X.data_ptr(), shape, args.precision, ctx=ctx)
+    loss = None
+    for _ in range(args.warmup + args.launches):
+        loss = d.loss_grad_dev([f.data_ptr() for f in fs], args.rank, 1e-3,
+                               [g.data_ptr() for g in gs])
+    torch.cuda.synchronize()
+    print("loss_grad", args.precision, shape, "rank", args.rank, "loss", loss)
+    d.close()
+
+
+def case_batched(args):
+    """The 512-instance batched CP-ALS run (sizes U{16..96}, ranks U{4..16})."""
+    import torch
+
+    import tenrso_b200 as tb
+    from tenrso_b200 import synth
+    ctx = _ctx()
+    inst = synth.batched_instances(512, 0xC4)
+    b = tb.BatchedCpAls([X.astype(np.float32) for X, _, _ in inst], [R for _, R, _ in inst],
+                        ctx=ctx)
+    d_init = torch.from_numpy(b.pack([i for _, _, i in inst])).cuda()
+    d_out = torch.empty_like(d_init)
+    torch.cuda.synchronize()
+    info = None
+    for _ in range(args.warmup + args.launches):
+        info = b.cp_als_dev(args.iters, 0.0, d_init.data_ptr(), d_out.data_ptr(), want_info=True)
+    print("batched", len(inst), "instances", args.iters, "iterations, mean fit",
+          float(np.mean([f for f, _, _ in info])), b.config)
+    b.close()
+
+
+CASES = {"mttkrp": case_mttkrp, "cp_als": case_cp_als, "csf_mttkrp": case_csf_mttkrp,
+         "loss_grad": case_loss_grad, "batched": case_batched}
 
 
 def main(argv=None):

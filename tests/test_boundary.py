@@ -116,3 +116,16 @@ def test_cp_reconstruction_grad_errors():
     one = tb.CpReconstructionGrad([np.ones((3, 2), np.float32)])
     with pytest.raises(tb.TenrsoError, match="Need at least one factor for Khatri-Rao product"):
         one.compute_factor_gradients(np.ones((3,), np.float32))
+
+
+def test_batched_validation():
+    X = np.ones((4, 5, 6), np.float32)
+    with pytest.raises(tb.TenrsoError, match="instance 1: Invalid rank: 5"):
+        tb.BatchedCpAls([X, X], [2, 5])
+    with pytest.raises(tb.TenrsoError, match="instance 0: Invalid rank: 0"):
+        tb.BatchedCpAls([X], [0])
+    Y = np.ones((20, 20, 20), np.float32)
+    with pytest.raises(tb.TenrsoError, match="rank <= 16"):
+        tb.BatchedCpAls([Y], [17])
+    with pytest.raises(ValueError, match="3-way"):
+        tb.BatchedCpAls([np.ones((3, 3), np.float32)], [1])
