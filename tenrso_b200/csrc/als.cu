@@ -96,99 +96,100 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
   }
 }
 
-// Block Gauss-Jordan inverse of the (padded) Hadamard G, no pivoting, 16 x 16
-// pivot blocks. Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and
-// columns tx + 16b (RB x RB doubles in registers). Block step K:
-//   P = G[K][K] is inverted by warp 0 (scalar Gauss-Jordan in shared memory,
-//     __syncwarp between its 16 pivots);
-//   G[K][j] <- P^-1 G[K][j],  G[i][K] <- -G[i][K] P^-1,
-//   G[i][j] <- G[i][j] - G[i][K] P^-1 G[K][j],  G[K][K] <- P^-1.
-// After the last block G holds G^-1. Every scalar pivot met on the way is a
-// pivot of G's LDL^T factorisation, so all are positive iff G is SPD; a pivot
-// that is not positive or not finite reports "not SPD" (uniform across the CTA).
+// Gauss-Jordan inverse of the (padded) Hadamard G, one pivot per step, no
+// pivoting. Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns
+// tx + 16b (RB x RB doubles in registers). Step k reads row k and column k
+// (published by their owners at the end of step k-1 into a double buffer) and
+// updates every element branch-free,
+//   A[i][j] <- A[i][j] - (A[i][k] / p) A[k][j],
+// after which the owners of row k and column k overwrite them:
+//   A[k][j] <- A[k][j] / p,  A[i][k] <- -A[i][k] / p,  A[k][k] <- 1 / p.
+// One barrier per step. Every pivot met on the way is a pivot of G's LDL^T
+// factorisation, so all are positive iff G is SPD; a pivot that is not
+// positive or not finite reports "not SPD" (uniform: all threads read it).
 template <int RB>
 struct GjShared {
-  double P[16][17];
-  double rowK[16][16 * RB];
-  double rowK2[16][16 * RB];
-  double colK[16 * RB][17];
+  double row[2][16 * RB];
+  double col[2][16 * RB];
   double scale;
-  int bad;
 };
 
+// 1/p by Newton-Raphson refinement x <- x (2 - p x) of a single-precision
+// seed (two steps: about 23 -> 46 -> 92 correct bits before FP64 rounding).
+// Called for positive pivots inside float's normal range.
+__device__ __forceinline__ double recip_nr(double p) {
+  double x = (double)(1.0f / (float)p);
+  x = x * fma(-p, x, 2.0);
+  x = x * fma(-p, x, 2.0);
+  return x;
+}
+
 template <int RB>
-__device__ bool gj_inverse_block(double (&a)[RB][RB], GjShared<RB>& sh) {
+__device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
+  constexpr int N = 16 * RB;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) sh.bad = 0;
+  // publish row 0 and column 0
+  if (ty == 0) {
 #pragma unroll
-  for (int K = 0; K < RB; ++K) {
-    // publish row block K, column block K and the pivot block
+    for (int bj = 0; bj < RB; ++bj) sh.row[0][tx + 16 * bj] = a[0][bj];
+  }
+  if (tx == 0) {
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) sh.rowK[ty][tx + 16 * bj] = a[K][bj];
+    for (int ai = 0; ai < RB; ++ai) sh.col[0][ty + 16 * ai] = a[ai][0];
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < N; ++k) {
+    const int buf = k & 1;
+    const double p = sh.row[buf][k];
+    if (!(p > 0.0) || !isfinite(p)) return false;
+    const double inv = (p > 1e-30 && p < 1e30) ? recip_nr(p) : 1.0 / p;
+    const int kb = k >> 4, kl = k & 15;
+    const int n1 = k + 1, n1b = n1 >> 4, n1l = n1 & 15;
+    double rk[RB], ck[RB];
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai) sh.colK[ty + 16 * ai][tx] = a[ai][K];
-    sh.P[ty][tx] = a[K][K];
-    __syncthreads();
-    if (warp == 0) {
-      double v[8];
-      const int c = lane & 15, r0 = lane >> 4;
+    for (int bj = 0; bj < RB; ++bj) rk[bj] = sh.row[buf][tx + 16 * bj];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = sh.P[r0 + 2 * q][c];
-      const bool ok = warp_gj16(v, lane);
+    for (int ai = 0; ai < RB; ++ai) ck[ai] = sh.col[buf][ty + 16 * ai] * inv;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) sh.P[r0 + 2 * q][c] = v[q];
-      if (lane == 0 && !ok) sh.bad = 1;
+    for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) a[ai][bj] = fma(-ck[ai], rk[bj], a[ai][bj]);
+    if (ty == kl) {
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+        if (ai == kb) {
+#pragma unroll
+          for (int bj = 0; bj < RB; ++bj) a[ai][bj] = rk[bj] * inv;
+        }
     }
-    __syncthreads();
-    if (sh.bad) return false;  // uniform: read after the barrier
-    // rowK2 = P^-1 . G[K][:] for the row-block-K rows this thread owns
-    {
-      double acc[RB];
+    if (tx == kl) {
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) acc[bj] = 0.0;
+      for (int bj = 0; bj < RB; ++bj)
+        if (bj == kb) {
 #pragma unroll
-      for (int m = 0; m < 16; ++m) {
-        const double pm = sh.P[ty][m];
+          for (int ai = 0; ai < RB; ++ai) a[ai][bj] = (ty + 16 * ai == k) ? inv : -ck[ai];
+        }
+    }
+    if (n1 < N) {
+      if (ty == n1l) {
 #pragma unroll
-        for (int bj = 0; bj < RB; ++bj) acc[bj] += pm * sh.rowK[m][tx + 16 * bj];
+        for (int ai = 0; ai < RB; ++ai)
+          if (ai == n1b) {
+#pragma unroll
+            for (int bj = 0; bj < RB; ++bj) sh.row[buf ^ 1][tx + 16 * bj] = a[ai][bj];
+          }
       }
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj) sh.rowK2[ty][tx + 16 * bj] = acc[bj];
-    }
-    __syncthreads();
-    // rank-16 update, register blocked: per m, RB + RB shared loads feed
-    // RB x RB FMAs
-    double colacc[RB];
-#pragma unroll
-    for (int ai = 0; ai < RB; ++ai) colacc[ai] = 0.0;
-#pragma unroll
-    for (int m = 0; m < 16; ++m) {
-      double x[RB], y[RB];
-#pragma unroll
-      for (int ai = 0; ai < RB; ++ai) x[ai] = sh.colK[ty + 16 * ai][m];
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj) y[bj] = sh.rowK2[m][tx + 16 * bj];
-      const double pmx = sh.P[m][tx];
-#pragma unroll
-      for (int ai = 0; ai < RB; ++ai) {
-        colacc[ai] += x[ai] * pmx;
+      if (tx == n1l) {
 #pragma unroll
         for (int bj = 0; bj < RB; ++bj)
-          if (ai != K && bj != K) a[ai][bj] -= x[ai] * y[bj];
+          if (bj == n1b) {
+#pragma unroll
+            for (int ai = 0; ai < RB; ++ai) sh.col[buf ^ 1][ty + 16 * ai] = a[ai][bj];
+          }
       }
     }
-#pragma unroll
-    for (int ai = 0; ai < RB; ++ai) {
-      if (ai == K) {
-#pragma unroll
-        for (int bj = 0; bj < RB; ++bj)
-          a[ai][bj] = (bj == K) ? sh.P[ty][tx] : sh.rowK2[ty][tx + 16 * bj];
-      } else {
-        a[ai][K] = -colacc[ai];
-      }
-    }
-    __syncthreads();  // shared row/column blocks are rewritten by the next step
+    __syncthreads();
   }
   return true;
 }
@@ -249,11 +250,11 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
   load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
-  bool ok = gj_inverse_block<RB>(a, gsh);
+  bool ok = gj_inverse<RB>(a, gsh);
   if (!ok) {
     __syncthreads();
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
-    ok = gj_inverse_block<RB>(a, gsh);
+    ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
   }
   if (!ok) {
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
     __syncthreads();
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps * fmax(gsh.scale, 1.0),
                       a, false);
-    ok = gj_inverse_block<RB>(a, gsh);
+    ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 2;
   }
   if (!ok) {

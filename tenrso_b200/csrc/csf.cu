@@ -386,7 +386,7 @@ struct Csf3Args {
   const float* Ua;  // level-1 factor
   const float* Ub;  // leaf factor
   int R;
-  float* M;
+  double* M;        // FP64 output accumulator (rows of the root mode)
 };
 
 // One warp owns a task of 1024 consecutive entries and walks it in batches
@@ -443,7 +443,7 @@ struct CsfSlots {
 // Sum the per-slot partial root sums of the lanes that share a column quad
 // and add them to output row `rid` (slot-0 lanes issue the atomics).
 template <int R>
-__device__ __forceinline__ void csf_flush(float4& acc, uint32_t rid, int lane, float* M) {
+__device__ __forceinline__ void csf_flush(float4& acc, uint32_t rid, int lane, double* M) {
   constexpr int LPR = CsfSlots<R>::LPR;
 #pragma unroll
   for (int o = LPR; o < 32; o <<= 1) {
@@ -452,7 +452,14 @@ __device__ __forceinline__ void csf_flush(float4& acc, uint32_t rid, int lane, f
     acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
     acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
   }
-  if (lane < LPR) atomicAdd(reinterpret_cast<float4*>(M + (size_t)rid * R) + lane, acc);
+  if (lane < LPR) {
+    // FP64 accumulation: heavy (Zipf-head) rows receive many task sums
+    double* o = M + (size_t)rid * R + 4 * lane;
+    atomicAdd(o + 0, (double)acc.x);
+    atomicAdd(o + 1, (double)acc.y);
+    atomicAdd(o + 2, (double)acc.z);
+    atomicAdd(o + 3, (double)acc.w);
+  }
   acc = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -571,7 +578,7 @@ struct CsfGenArgs {
   int root_mode;
   const float* U[kMaxModes];
   int R;
-  float* M;
+  double* M;
 };
 
 __global__ void csf_generic_mttkrp_kernel(CsfGenArgs a) {
@@ -592,8 +599,14 @@ __global__ void csf_generic_mttkrp_kernel(CsfGenArgs a) {
       else
         prod *= a.U[m][i * a.R + r];
     }
-    atomicAdd(a.M + root * a.R + r, prod);
+    atomicAdd(a.M + root * a.R + r, (double)prod);
   }
+}
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ in, int64_t n, float* __restrict__ out) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = (float)in[e];
 }
 
 template <int R>
@@ -611,11 +624,28 @@ void launch_csf3_slot(tsr_ctx* ctx, cudaStream_t s, const Csf3Args& a) {
 
 void init_csf_attributes() {}  // the CSF kernels use no dynamic shared memory
 
+int launch_csf_accumulate(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp,
+                          const FactorTable& ft, int R, int mode, double* d_out);
+
 int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const FactorTable& ft,
-                      int R, int mode, float* d_out) {
+                      int R, int mode, float* d_out, double* d_acc) {
   const CsfDev& c = sp->modes[mode];
-  TSR_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float) * sp->shape[mode] * R, s));
-  if (c.nnz == 0) return TSR_OK;
+  const int64_t n_out = sp->shape[mode] * R;
+  if (c.nnz == 0) {
+    TSR_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float) * n_out, s));
+    return TSR_OK;
+  }
+  TSR_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(double) * n_out, s));
+  TSR_TRY(launch_csf_accumulate(ctx, s, sp, ft, R, mode, d_acc));
+  f64_to_f32_kernel<<<grid_for(ctx, n_out), 256, 0, s>>>(d_acc, n_out, d_out);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_csf_accumulate(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp,
+                          const FactorTable& ft, int R, int mode, double* d_out) {
+  const CsfDev& c = sp->modes[mode];
   bool vec = R % 4 == 0 && R <= 128 && ((uintptr_t)d_out & 15) == 0;
   for (int m = 0; m < c.ndim && vec; ++m) vec = ((uintptr_t)ft.ptr[m] & 15) == 0;
   if (c.ndim == 3 && vec) {
@@ -943,7 +973,9 @@ int tsr_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, const float* cons
     ft.ptr[m] = d_factors[m];
     ft.rows[m] = sp->shape[m];
   }
-  return launch_mttkrp_csf(ctx, ctx->stream, sp, ft, (int)rank, mode, d_out);
+  void* acc;
+  TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(double) * sp->shape[mode] * rank, &acc));
+  return launch_mttkrp_csf(ctx, ctx->stream, sp, ft, (int)rank, mode, d_out, (double*)acc);
 }
 
 int tsr_mttkrp_csf_f32(tsr_ctx* ctx, const tsr_sparse* sp, const float* const* factors,

@@ -39,10 +39,11 @@ struct tsr_sparse {
 
 namespace tsr {
 
-// Sparse MTTKRP of `sp` rooted at `mode` into d_out (shape[mode] x R, zeroed
-// here). Factors are device pointers (row-major I_m x R).
+// Sparse MTTKRP of `sp` rooted at `mode` into d_out (shape[mode] x R fp32).
+// The sums accumulate in FP64 in d_acc (shape[mode] x R doubles, zeroed here)
+// and are rounded once into d_out. Factors are device pointers (I_m x R).
 int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const FactorTable& ft,
-                      int R, int mode, float* d_out);
+                      int R, int mode, float* d_out, double* d_acc);
 // Shared-memory limits of the CSF kernels (once per process, before capture).
 void init_csf_attributes();
 

@@ -225,6 +225,7 @@ struct SweepArgs {
   float* partials;
   AlsBuffers b;
   const tsr_sparse* sp;  // sparse source (CSF MTTKRP) instead of the dense unfoldings
+  double* acc64;         // sparse: FP64 accumulator of the CSF MTTKRP
 };
 
 static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<ModeOperand>& ops) {
@@ -238,7 +239,7 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
     float* partials = a.partials;
     int splits = 1;
     if (a.sp)
-      TSR_TRY(launch_mttkrp_csf(ctx, A, a.sp, a.ft, a.R, n, partials));
+      TSR_TRY(launch_mttkrp_csf(ctx, A, a.sp, a.ft, a.R, n, partials, a.acc64));
     else
       TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
     TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
@@ -322,6 +323,9 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     void* pp;
     TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
     a.partials = (float*)pp;
+    void* ap;
+    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(double) * pmax, &ap));
+    a.acc64 = (double*)ap;
   } else if (max_iters > 0) {
     for (int m = 0; m < ndim; ++m) {
       TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));

@@ -7,6 +7,7 @@ namespace tsr {
 struct SplitPlan {
   int splits = 1;
   int64_t k_per_split = 0;
+  int bn = 64;  // FP32 path: output columns per CTA tile (32 or 64)
 };
 
 void init_tc_attributes();

@@ -13,16 +13,35 @@
 namespace tsr {
 
 namespace {
-constexpr int BM = 128, BN = 64, BK = 32, NT = 256;
+constexpr int BK = 32;
 
-__global__ void __launch_bounds__(NT, 2)
+template <int BM, int BN>
+constexpr int simt_threads() {
+  return (BM / 8) * (BN / 4);
+}
+template <int BM, int BN>
+constexpr int simt_min_blocks() {
+  return 512 / simt_threads<BM, BN>() > 4 ? 4 : 512 / simt_threads<BM, BN>();
+}
+
+// BM x BN output tile per CTA, 8 x 4 per thread; NPF factor rows of each KR
+// row are loaded one K-step ahead (the rest, for tensors of more than NPF + 1
+// modes, after the FMA loop).
+template <int BM, int BN, int NPF>
+__global__ void __launch_bounds__(simt_threads<BM, BN>(), simt_min_blocks<BM, BN>())
 mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, int64_t ld,
                          KRSpec kr, int64_t k_per_split, float* __restrict__ partials) {
+  constexpr int NT = simt_threads<BM, BN>();
+  constexpr int A_IT = BM * BK / 4 / NT;  // float4 of the A tile per thread
+  constexpr int B_TPR = BN / 8;            // threads per KR row (8 columns each)
+  constexpr int B_RPP = NT / B_TPR;        // KR rows per pass
+  constexpr int B_IT = BK / B_RPP;         // passes per K-step
+  static_assert(B_IT >= 1 && BK % B_RPP == 0, "tile");
   extern __shared__ __align__(16) float simt_smem[];
   float(*As)[BK][BM + 4] = reinterpret_cast<float(*)[BK][BM + 4]>(simt_smem);
   float(*Bs)[BK][BN] = reinterpret_cast<float(*)[BK][BN]>(simt_smem + 2 * BK * (BM + 4));
   const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
+  const int tx = tid % (BN / 4), ty = tid / (BN / 4);
   const int64_t m0 = (int64_t)blockIdx.y * BM;
   const int n0 = blockIdx.z * BN;
   const int R = kr.R;
@@ -36,12 +55,12 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
 
-  float4 areg[4];
-  float breg[8];
-  // A-tile mapping: 8 threads per row (32 floats = 128 B), 32 rows per pass.
+  float4 areg[A_IT];
+  float breg[B_IT][8];
+  // A-tile mapping: 8 threads per row (32 floats = 128 B).
   auto load_a = [&](int64_t k0) {
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < A_IT; ++it) {
       int idx = it * NT + tid;
       int m = idx / 8, kq = idx % 8;
       int64_t gm = m0 + m, gk = k0 + kq * 4;
@@ -58,7 +77,7 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
   };
   auto store_a = [&](int buf) {
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < A_IT; ++it) {
       int idx = it * NT + tid;
       int m = idx / 8, kq = idx % 8;
       As[buf][kq * 4 + 0][m] = areg[it].x;
@@ -67,42 +86,55 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
       As[buf][kq * 4 + 3][m] = areg[it].w;
     }
   };
-  // B-tile mapping: thread -> (kk = tid / 8, 8 consecutive columns). The
-  // factor values of the next K-step are loaded before the FMA loop of the
-  // current one and multiplied after it, so the L2 latency overlaps the math.
-  float braw[2][8];
-  uint32_t boff[kMaxModes];
-  bool bvalid = false;
+  // B-tile mapping: thread -> (KR row kk, 8 consecutive columns). The factor
+  // values of the next K-step are loaded before the FMA loop of the current
+  // one and multiplied after it, so the L2 latency overlaps the math.
+  float braw[B_IT][NPF][8];
+  uint32_t boff[B_IT][kMaxModes];
+  bool bvalid[B_IT];
   auto gen_b_load = [&](int64_t k0) {
-    const int kk = tid / 8, c0 = (tid % 8) * 8;
-    const int64_t j = k0 + kk;
-    bvalid = j < kend;
-    kr_row_offsets(kr, (uint32_t)(bvalid ? j : kbeg), boff);
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int c = n0 + c0 + e;
-      const int cc = c < R ? c : 0;
-      braw[0][e] = __ldg(kr.f[0] + boff[0] + cc);
-      braw[1][e] = kr.n_other > 1 ? __ldg(kr.f[1] + boff[1] + cc) : 1.f;
+    for (int bi = 0; bi < B_IT; ++bi) {
+      const int kk = bi * B_RPP + tid / B_TPR, c0 = (tid % B_TPR) * 8;
+      const int64_t j = k0 + kk;
+      bvalid[bi] = j < kend;
+      kr_row_offsets(kr, (uint32_t)(bvalid[bi] ? j : kbeg), boff[bi]);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int c = n0 + c0 + e;
+        const int cc = c < R ? c : 0;
+#pragma unroll
+        for (int q = 0; q < NPF; ++q)
+          braw[bi][q][e] = q < kr.n_other ? __ldg(kr.f[q] + boff[bi][q] + cc) : 1.f;
+      }
     }
   };
   auto gen_b_finish = [&]() {
-    const int c0 = (tid % 8) * 8;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int c = n0 + c0 + e;
-      float v = braw[0][e] * braw[1][e];
+    for (int bi = 0; bi < B_IT; ++bi) {
+      const int c0 = (tid % B_TPR) * 8;
 #pragma unroll
-      for (int q = 2; q < kMaxModes; ++q)
-        if (q < kr.n_other) v *= __ldg(kr.f[q] + boff[q] + (c < R ? c : 0));
-      breg[e] = (bvalid && c < R) ? v : 0.f;
+      for (int e = 0; e < 8; ++e) {
+        const int c = n0 + c0 + e;
+        float v = braw[bi][0][e];
+#pragma unroll
+        for (int q = 1; q < NPF; ++q) v *= braw[bi][q][e];
+#pragma unroll
+        for (int q = NPF; q < kMaxModes; ++q)
+          if (q < kr.n_other) v *= __ldg(kr.f[q] + boff[bi][q] + (c < R ? c : 0));
+        breg[bi][e] = (bvalid[bi] && c < R) ? v : 0.f;
+      }
     }
   };
   auto store_b = [&](int buf) {
-    int kk = tid / 8, c0 = (tid % 8) * 8;
-    *reinterpret_cast<float4*>(&Bs[buf][kk][c0]) = make_float4(breg[0], breg[1], breg[2], breg[3]);
-    *reinterpret_cast<float4*>(&Bs[buf][kk][c0 + 4]) =
-        make_float4(breg[4], breg[5], breg[6], breg[7]);
+#pragma unroll
+    for (int bi = 0; bi < B_IT; ++bi) {
+      const int kk = bi * B_RPP + tid / B_TPR, c0 = (tid % B_TPR) * 8;
+      *reinterpret_cast<float4*>(&Bs[buf][kk][c0]) =
+          make_float4(breg[bi][0], breg[bi][1], breg[bi][2], breg[bi][3]);
+      *reinterpret_cast<float4*>(&Bs[buf][kk][c0 + 4]) =
+          make_float4(breg[bi][4], breg[bi][5], breg[bi][6], breg[bi][7]);
+    }
   };
 
   if (nsteps > 0) {
@@ -208,17 +240,30 @@ int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, i
   return TSR_OK;
 }
 
+template <int BM, int BN>
+constexpr size_t simt_smem_bytes() {
+  return sizeof(float) * 2 * BK * (BM + 4 + BN);
+}
+
 void init_simt_attributes() {
-  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(float) * 2 * BK * (BM + 4 + BN)));
+  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 64, 2>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 64>());
+  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 64, 4>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 64>());
+  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 32, 2>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 32>());
+  cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 32, 4>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 32>());
 }
 
 SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
   SplitPlan p;
-  int64_t mt = ceil_div(rows, BM), nt = ceil_div(R, BN);
-  // one full wave at two resident CTAs per SM (no tail wave)
+  p.bn = R <= 32 ? 32 : 64;
+  const int64_t mt = ceil_div(rows, 128), nt = ceil_div(R, p.bn);
+  // one full wave at the resident CTAs per SM (2 of 256 threads, 4 of 128)
+  const int per_sm = p.bn == 32 ? 4 : 2;
   int64_t want =
-      std::max<int64_t>(1, (int64_t)(ctx->sm_count - ctx->reserve_sms) * 2 / (mt * nt));
+      std::max<int64_t>(1, (int64_t)(ctx->sm_count - ctx->reserve_sms) * per_sm / (mt * nt));
   int64_t steps = ceil_div(K, BK);
   want = std::min<int64_t>(want, steps);
   p.k_per_split = round_up(ceil_div(K, want), BK);
@@ -226,14 +271,28 @@ SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
   return p;
 }
 
+template <int BM, int BN, int NPF>
+void launch_simt_tile(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
+                      const SplitPlan& plan, float* partials, dim3 grid) {
+  mttkrp_f32_splitk_kernel<BM, BN, NPF>
+      <<<grid, simt_threads<BM, BN>(), simt_smem_bytes<BM, BN>(), ctx->stream>>>(
+          A, u.rows, u.cols, u.ld, kr, plan.k_per_split, partials);
+}
+
 int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
                        const SplitPlan& plan, float* partials) {
   if (u.cols >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "unfolding too wide");
-  dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, BM), (unsigned)ceil_div(kr.R, BN));
+  const int bn = plan.bn == 32 ? 32 : 64;
+  dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, 128), (unsigned)ceil_div(kr.R, bn));
   if (grid.y > 65535 || grid.z > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
-  const size_t smem = sizeof(float) * 2 * BK * (BM + 4 + BN);
-  mttkrp_f32_splitk_kernel<<<grid, NT, smem, ctx->stream>>>(A, u.rows, u.cols, u.ld, kr,
-                                                            plan.k_per_split, partials);
+  const bool wide = kr.n_other > 2;
+  if (bn == 32) {
+    if (wide) launch_simt_tile<128, 32, 4>(ctx, A, u, kr, plan, partials, grid);
+    else launch_simt_tile<128, 32, 2>(ctx, A, u, kr, plan, partials, grid);
+  } else {
+    if (wide) launch_simt_tile<128, 64, 4>(ctx, A, u, kr, plan, partials, grid);
+    else launch_simt_tile<128, 64, 2>(ctx, A, u, kr, plan, partials, grid);
+  }
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
