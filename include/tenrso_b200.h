@@ -146,7 +146,7 @@ int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
                                  const int64_t* shape, const float* const* d_factors,
                                  int64_t rank, float* d_out);
 
-/* ---- CP-ALS: crates/tenrso-decomp/src/cp/core.rs:91-214 -----------------
+/* ---- CP-ALS: crates/tenrso-decomp/src/cp/core.rs:59-182 -----------------
  * Same loop, validation (rank in [1, min I_n], tol in [0,1)), fit, oscillation
  * and convergence rules. init_factors: concatenated row-major I_0xR, I_1xR, ...
  * (the injected initialisation tenrso cannot seed); NULL = U(0,1) from the
@@ -214,7 +214,7 @@ int tsr_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, const float* cons
 int tsr_profile_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp,
                                    const float* const* d_factors, int64_t rank, int mode,
                                    int iters, int flush_l2, double* ms_per_launch);
-/* Sparse CP-ALS (tenrso has none): cp_als's loop (cp/core.rs:91-214) with the
+/* Sparse CP-ALS (tenrso has none): cp_als's loop (cp/core.rs:59-182) with the
  * CSF MTTKRP; FP32 factors, FP64 Gram/solve/fit. */
 int tsr_cp_als_sparse_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
                           double tol, const float* init_factors, uint64_t seed,
@@ -269,7 +269,7 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
                              int64_t rank, double reg, float* const* d_grads, double* loss);
 
 /* ---- batched CP-ALS (no tenrso counterpart; each instance is cp_als,
- * crates/tenrso-decomp/src/cp/core.rs:91-214, from injected factors) -------
+ * crates/tenrso-decomp/src/cp/core.rs:59-182, from injected factors) -------
  * A device-resident batch of n_inst dense 3-way tensors: shapes is n_inst x 3,
  * ranks n_inst (1 <= rank <= min(shape), rank <= 16), tensors[b] a host
  * row-major fp32 tensor. Factors of the whole batch are one packed array:

@@ -275,7 +275,7 @@ T compute_fit(const T* X, int ndim, const i64* shape, const std::vector<std::vec
   return std::min(std::max(fit, T(0)), T(1));
 }
 
-// crates/tenrso-decomp/src/cp/core.rs:91-214 (cp_als) with the factors
+// crates/tenrso-decomp/src/cp/core.rs:59-182 (cp_als) with the factors
 // injected instead of thread_rng (helpers.rs:212-222 cannot be seeded).
 // reason: 0 MaxIterations, 1 FitTolerance, 2 Oscillation.
 template <class T>
@@ -414,7 +414,7 @@ int orc_cp_als_f64(const double* X, int ndim, const int64_t* shape, int64_t R, i
                              reason, osc, final_change, fit, faithful);
 }
 
-// One mode update of the reference loop (core.rs:161-171) in T=double, used to
+// One mode update of the reference loop (core.rs:129-140) in T=double, used to
 // check the GPU solve in isolation: U_mode <- mttkrp * gram_hadamard^-1.
 int orc_solve_f64(const double* M, int64_t rows, const double* G, int64_t R, double* out) {
   std::vector<double> g(G, G + R * R);

@@ -125,7 +125,7 @@ REASONS = ("MaxIterations", "FitTolerance", "Oscillation", "TimeLimit")
 
 def cp_als(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
            faithful: bool = False):
-    """Restated ``tenrso_decomp::cp_als`` (cp/core.rs:91-214) from injected
+    """Restated ``tenrso_decomp::cp_als`` (cp/core.rs:59-182) from injected
     factors. Returns (factors, info dict)."""
     dt = X.dtype
     X = np.ascontiguousarray(X)

@@ -1,6 +1,6 @@
 """Batched CP-ALS over the C ABI: many independent 3-way instances of uneven
 shape and rank in one persistent launch. Each instance follows tenrso's
-cp_als (crates/tenrso-decomp/src/cp/core.rs:91-214) from its own initial
+cp_als (crates/tenrso-decomp/src/cp/core.rs:59-182) from its own initial
 factors; tenrso itself has no batched entry point (it would loop cp_als).
 
 Factors of the whole batch live in one packed float32 array: instance b at

@@ -2,7 +2,7 @@
 //   compute_gram_matrix / compute_gram_hadamard   helpers.rs:409-452
 //   solve_least_squares (per-row lstsq + ridge)   helpers.rs:455-495
 //   compute_norm_squared / compute_fit            helpers.rs:498-579
-//   convergence + oscillation bookkeeping          core.rs:173-198
+//   convergence + oscillation bookkeeping          core.rs:142-166
 // The per-row least-squares solves become one in-place Gauss-Jordan inverse of
 // the symmetric Gram G (FP64, no pivoting: every pivot of an SPD matrix is
 // positive, so a non-positive pivot is the "not SPD" signal that triggers the
@@ -387,7 +387,7 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
   const double err = sqrt(fmax(err_sq, 0.0));
   double fit = 1.0 - err / sqrt(xn);
   fit = fmin(fmax(fit, 0.0), 1.0);
-  // core.rs:173-198
+  // core.rs:142-166
   const int iter = st->iter;
   st->fit = fit;
   b.history[iter] = fit;

@@ -6,7 +6,7 @@ namespace tsr {
 
 constexpr int kMaxRank = 112;  // two R x R FP64 matrices fit in shared memory
 
-// Device-resident ALS bookkeeping mirroring cp/core.rs:104-198.
+// Device-resident ALS bookkeeping mirroring cp/core.rs:101-166.
 struct AlsState {
   double xnorm_sq;      // ||X||^2 (FP64)
   double inner;         // <X, Xhat> accumulated by the last mode's solve
@@ -73,7 +73,7 @@ int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int
 // U_mode = (sum of split partials) . G^{-1}; `last` accumulates <M, U>.
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, bool last);
-// fit, fit_history, oscillation and convergence rules of cp/core.rs:173-198.
+// fit, fit_history, oscillation and convergence rules of cp/core.rs:142-166.
 int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol);
 
 }  // namespace tsr

@@ -1,9 +1,9 @@
 // Batched CP-ALS: many independent 3-way instances of uneven shape and rank
 // in one persistent launch. Each instance runs tenrso's cp_als loop
-// (crates/tenrso-decomp/src/cp/core.rs:91-214) from its own injected factors:
+// (crates/tenrso-decomp/src/cp/core.rs:59-182) from its own injected factors:
 // the same mode order, Gram-Hadamard solve with the reference's ridge
 // fallback (cp/helpers.rs:455-495), fit (helpers.rs:513-530) and
-// convergence / oscillation rules (core.rs:173-198).
+// convergence / oscillation rules (core.rs:142-166).
 //
 // Design:
 //  - one CTA owns one instance at a time and keeps its three factors (fp32)
@@ -383,7 +383,7 @@ __device__ void run_instance(const BatchArgs& a, int id, unsigned char* smem_raw
       __syncthreads();
       break;
     }
-    // ---- fit (helpers.rs:513-530) and the rules of core.rs:173-198
+    // ---- fit (helpers.rs:513-530) and the rules of core.rs:142-166
     double inner = 0.0;
     for (int e = threadIdx.x; e < n2 * Rp; e += NT)
       inner += (double)s.M[e] * (double)s.C[e];
@@ -532,7 +532,7 @@ int batch_validate(int n_inst, const int64_t* shapes, const int64_t* ranks) {
       if (sh[m] <= 0)
         return fail(TSR_E_SHAPE, "instance %d: mode %d has size %lld", b, m, (long long)sh[m]);
     const int64_t R = ranks[b];
-    // core.rs:115-121
+    // core.rs:82-90
     if (R == 0 || R > std::min(sh[0], std::min(sh[1], sh[2])))
       return fail(TSR_E_INVALID_RANK, "instance %d: Invalid rank: %lld", b, (long long)R);
     if (R > kBatchMaxR)

@@ -1,7 +1,7 @@
 // Host mirror of tenrso's dense CP-ALS entry points over the C ABI:
 //   tenrso_kernels::khatri_rao       khatri_rao.rs:56-89
 //   tenrso_kernels::mttkrp (+blocked, all_modes)  mttkrp.rs:74-146, 395-498; utils.rs:282-307
-//   tenrso_decomp::cp_als            cp/core.rs:91-214
+//   tenrso_decomp::cp_als            cp/core.rs:59-182
 // Validation order and messages follow the cited lines so that a Rust shim can
 // surface them through anyhow / CpError unchanged.
 #include <chrono>
@@ -203,7 +203,7 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
 }
 
 // ---------------------------------------------------------------------------
-// CP-ALS driver (cp/core.rs:91-214) on a device-resident tensor.
+// CP-ALS driver (cp/core.rs:59-182) on a device-resident tensor.
 //
 // One ALS sweep runs on two streams so that the FP64 work overlaps the
 // MTTKRPs: the main stream carries MTTKRP_n -> solve_n, the aux stream
@@ -261,7 +261,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
                   const float* d_init, int precision, double time_limit_s, float* d_out,
                   tsr_cp_info* info) {
   auto t_start = std::chrono::steady_clock::now();
-  // core.rs:115-127
+  // core.rs:82-94
   if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
   for (int d = 0; d < ndim; ++d)
     if (rank > shape[d]) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
@@ -384,7 +384,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
       TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
       TSR_CUDA(cudaStreamSynchronize(ctx->stream));
       if (hs.done) break;
-      // core.rs:151-156: checked at the start of every iteration
+      // core.rs:118-124: checked at the start of every iteration
       const double el =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
       if (el > time_limit_s) {

@@ -4,7 +4,7 @@ Names, argument meaning and error behaviour follow the Rust functions:
   khatri_rao                  crates/tenrso-kernels/src/khatri_rao.rs:56-89 (panics -> raises)
   mttkrp / mttkrp_blocked ... crates/tenrso-kernels/src/mttkrp.rs:74-146, 395-992
   mttkrp_all_modes            crates/tenrso-kernels/src/utils.rs:282-307
-  cp_als / CpDecomp / ConvergenceInfo  crates/tenrso-decomp/src/cp/core.rs:91-214, types.rs:311-368
+  cp_als / CpDecomp / ConvergenceInfo  crates/tenrso-decomp/src/cp/core.rs:59-182, types.rs:311-368
 """
 from __future__ import annotations
 
