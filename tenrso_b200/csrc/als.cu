@@ -96,21 +96,30 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
   }
 }
 
-// Gauss-Jordan inverse of the (padded) Hadamard G, one pivot per step, no
-// pivoting. Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns
-// tx + 16b (RB x RB doubles in registers). Step k reads row k and column k
-// (published by their owners at the end of step k-1 into a double buffer) and
-// updates every element branch-free,
-//   A[i][j] <- A[i][j] - (A[i][k] / p) A[k][j],
-// after which the owners of row k and column k overwrite them:
-//   A[k][j] <- A[k][j] / p,  A[i][k] <- -A[i][k] / p,  A[k][k] <- 1 / p.
-// One barrier per step. Every pivot met on the way is a pivot of G's LDL^T
-// factorisation, so all are positive iff G is SPD; a pivot that is not
-// positive or not finite reports "not SPD" (uniform: all threads read it).
+// Gauss-Jordan inverse of the (padded) Hadamard G as N uniform rank-1
+// updates, no pivoting.
+//
+// G is first scaled to unit diagonal, G' = D G D with D = diag(1/sqrt(G_ii)),
+// so that G^-1 = D G'^-1 D and every pivot lies in (0, 1] (for an SPD matrix
+// the pivots are the LDL^T pivots, which never exceed the diagonal). One
+// Gauss-Jordan step k with pivot p is then exactly
+//   A <- A - u w^T,  u = column k of A except u_k = p - 1,
+//                    w = (row k of A except w_k = p + 1) / p,
+// which yields the pivot row A_kj / p, the pivot column -A_ik / p and the
+// corner 1 / p without special cases; with p <= 1 the +-1 terms do not cancel.
+// After steps 0..k-1 the matrix is symmetric within the processed and within
+// the unprocessed indices and antisymmetric across them, so column k is row k
+// with the sign of its processed entries flipped: each step needs only row k,
+// published by its owners into a double buffer, and one barrier.
+//
+// Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
+// (RB x RB doubles in registers). A pivot that is not positive or not finite
+// (including a non-positive diagonal) reports "not SPD"; every thread reads
+// the same pivot, so the decision is uniform.
 template <int RB>
 struct GjShared {
-  double row[2][16 * RB];
-  double col[2][16 * RB];
+  double row[2][16 * RB];  // pivot row of the current step (double buffered)
+  double dsc[16 * RB];     // the diagonal scaling 1 / sqrt(G_ii)
   double scale;
 };
 
@@ -128,14 +137,29 @@ template <int RB>
 __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
   constexpr int N = 16 * RB;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  // publish row 0 and column 0
+  // diagonal scaling (a non-positive diagonal scales its row to zero, whose
+  // pivot then reports "not SPD")
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj)
+      if (ty + 16 * ai == tx + 16 * bj) {
+        const double g = a[ai][bj];
+        sh.dsc[ty + 16 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
+      }
+  __syncthreads();
+  double di[RB], dj[RB];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai) di[ai] = sh.dsc[ty + 16 * ai];
+#pragma unroll
+  for (int bj = 0; bj < RB; ++bj) dj[bj] = sh.dsc[tx + 16 * bj];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
   if (ty == 0) {
 #pragma unroll
     for (int bj = 0; bj < RB; ++bj) sh.row[0][tx + 16 * bj] = a[0][bj];
-  }
-  if (tx == 0) {
-#pragma unroll
-    for (int ai = 0; ai < RB; ++ai) sh.col[0][ty + 16 * ai] = a[ai][0];
   }
   __syncthreads();
 #pragma unroll 1
@@ -143,54 +167,39 @@ __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
     const int buf = k & 1;
     const double p = sh.row[buf][k];
     if (!(p > 0.0) || !isfinite(p)) return false;
-    const double inv = (p > 1e-30 && p < 1e30) ? recip_nr(p) : 1.0 / p;
-    const int kb = k >> 4, kl = k & 15;
-    const int n1 = k + 1, n1b = n1 >> 4, n1l = n1 & 15;
-    double rk[RB], ck[RB];
+    const double inv = p > 1e-30 ? recip_nr(p) : 1.0 / p;
+    double u[RB], w[RB];
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) rk[bj] = sh.row[buf][tx + 16 * bj];
+    for (int ai = 0; ai < RB; ++ai) {
+      const int i = ty + 16 * ai;
+      const double r = sh.row[buf][i];
+      u[ai] = i == k ? p - 1.0 : (i < k ? -r : r);
+    }
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai) ck[ai] = sh.col[buf][ty + 16 * ai] * inv;
+    for (int bj = 0; bj < RB; ++bj) {
+      const int j = tx + 16 * bj;
+      const double r = sh.row[buf][j];
+      w[bj] = (j == k ? p + 1.0 : r) * inv;
+    }
 #pragma unroll
     for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) a[ai][bj] = fma(-ck[ai], rk[bj], a[ai][bj]);
-    if (ty == kl) {
+      for (int bj = 0; bj < RB; ++bj) a[ai][bj] = fma(-u[ai], w[bj], a[ai][bj]);
+    if (k + 1 < N) {
 #pragma unroll
       for (int ai = 0; ai < RB; ++ai)
-        if (ai == kb) {
+        if (ty + 16 * ai == k + 1) {
 #pragma unroll
-          for (int bj = 0; bj < RB; ++bj) a[ai][bj] = rk[bj] * inv;
+          for (int bj = 0; bj < RB; ++bj) sh.row[buf ^ 1][tx + 16 * bj] = a[ai][bj];
         }
-    }
-    if (tx == kl) {
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj)
-        if (bj == kb) {
-#pragma unroll
-          for (int ai = 0; ai < RB; ++ai) a[ai][bj] = (ty + 16 * ai == k) ? inv : -ck[ai];
-        }
-    }
-    if (n1 < N) {
-      if (ty == n1l) {
-#pragma unroll
-        for (int ai = 0; ai < RB; ++ai)
-          if (ai == n1b) {
-#pragma unroll
-            for (int bj = 0; bj < RB; ++bj) sh.row[buf ^ 1][tx + 16 * bj] = a[ai][bj];
-          }
-      }
-      if (tx == n1l) {
-#pragma unroll
-        for (int bj = 0; bj < RB; ++bj)
-          if (bj == n1b) {
-#pragma unroll
-            for (int ai = 0; ai < RB; ++ai) sh.col[buf ^ 1][ty + 16 * ai] = a[ai][bj];
-          }
-      }
     }
     __syncthreads();
   }
+  // G^-1 = D G'^-1 D
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
   return true;
 }
 
