@@ -172,7 +172,7 @@ int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& 
   bool tc = precision == TSR_PREC_BF16X3;
   if (tc && !tc_supported(op.u, R))
     return fail(TSR_E_UNSUPPORTED, "BF16X3 path needs rank <= 256 (got %d)", R);
-  plan = tc ? plan_tc(ctx, op.u.rows, op.u.cols, R) : plan_simt(ctx, op.u.rows, op.u.cols, R);
+  plan = tc ? plan_tc(ctx, op.u, R) : plan_simt(ctx, op.u.rows, op.u.cols, R);
   void* p;
   TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * partial_floats(plan, op.u.rows, R), &p));
   if (tc)
@@ -330,7 +330,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     for (int m = 0; m < ndim; ++m) {
       TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
       const bool tc = precision == TSR_PREC_BF16X3;
-      SplitPlan p = tc ? plan_tc(ctx, ops[m].u.rows, ops[m].u.cols, R)
+      SplitPlan p = tc ? plan_tc(ctx, ops[m].u, R)
                        : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
       pmax = std::max(pmax, partial_floats(p, ops[m].u.rows, R));
       a.op_ptrs[3 * m] = ops[m].f32;

@@ -8,6 +8,7 @@ struct SplitPlan {
   int splits = 1;
   int64_t k_per_split = 0;
   int bn = 64;  // FP32 path: output columns per CTA tile (32 or 64)
+  int run_length = 0;  // BF16x3 path: > 0 selects the prefix-scaled kernel (runs of this length)
 };
 
 void init_tc_attributes();
@@ -25,7 +26,7 @@ int launch_mttkrp_reduce_scaled(tsr_ctx* ctx, const float* partials, int splits,
 // BF16x3 tcgen05 kernel (mttkrp_tc.cu). The unfolding halves hi/lo are bf16
 // with row stride u.ld (a multiple of 8 elements, 16 bytes).
 bool tc_supported(const Unfolding& u, int R);
-SplitPlan plan_tc(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
+SplitPlan plan_tc(const tsr_ctx* ctx, const Unfolding& u, int R);
 int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16* lo,
                      const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
                      float* partials);

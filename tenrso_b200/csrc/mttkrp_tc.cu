@@ -406,6 +406,312 @@ mttkrp_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Prefix-scaled variant. When the fastest other mode has size L (a multiple
+// of 64), the KR rows come in runs of L that share every slower mode's row:
+// run P is U_last (L x R) with its columns scaled by the weight vector
+//   w_P[n] = prod over the slower other modes q of U_q[i_q(P), n],
+// so  M = sum_P (X_P . U_last) diag(w_P)  with X_P the L unfolding columns of
+// run P. U_last is the same for every run: the producer warps write it once
+// per CTA as the swizzled bf16 hi/lo B operand (instead of one KR tile per
+// stage). Each run's X_P . U_last accumulates in TMEM (hi.hi and the two
+// correction products in separate accumulators, double buffered across
+// runs); the epilogue warps scale it by w_P and add it into registers.
+// Split-K boundaries fall on run boundaries.
+constexpr int TCS_MAX_RUNS = 16;  // runs per CTA (their weights sit in shared memory)
+constexpr int TCS_MAX_L = 384;    // U_last tiles must fit beside the stage ring
+
+struct TcsParams {
+  int64_t rows;
+  int64_t K;
+  int64_t k_per_split;  // a whole number of runs
+  int L;                // run length, multiple of 64
+  int n_pad;            // R rounded up to 16 (<= 64)
+  int acc_cols;         // TMEM columns per accumulator (power of two >= max(n_pad, 32))
+  int stages;
+  KRSpec kr;
+  float* partials;
+  unsigned* status;
+};
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
+                          const __grid_constant__ CUtensorMap map_lo, TcsParams p) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+  const int S = p.stages;
+  const int spr = p.L / TC_BK;                          // stages per run
+  const uint32_t bblk = (uint32_t)p.n_pad * 128u;       // one k-block of B (hi or lo)
+  uint8_t* a_base = smem;
+  uint8_t* b_base = smem + (size_t)S * 2 * A_TILE_BYTES;
+  float* wts = reinterpret_cast<float*>(b_base + (size_t)spr * 2 * bblk);  // [runs][64]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(wts + TCS_MAX_RUNS * 64);
+  uint64_t* tma_full = bars;
+  uint64_t* empty = bars + S;
+  uint64_t* acc_full = bars + 2 * S;   // [2]
+  uint64_t* acc_empty = bars + 2 * S + 2;  // [2]
+  uint64_t* b_ready = bars + 2 * S + 4;
+  uint64_t* mma_done = bars + 2 * S + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 6);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t m0 = (int64_t)blockIdx.y * TC_BM;
+  const int64_t kbeg = (int64_t)blockIdx.x * p.k_per_split;
+  const int64_t kend = min(p.K, kbeg + p.k_per_split);
+  const int nruns = kend > kbeg ? (int)((kend - kbeg) / p.L) : 0;
+  const int nsteps = nruns * spr;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&tma_full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);
+    }
+    mbar_init(b_ready, 4);
+    mbar_init(mma_done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    prefetch_tmap(&map_hi);
+    prefetch_tmap(&map_lo);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, (uint32_t)(4 * p.acc_cols));
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued_upto = 0;
+      for (int it = 0; it < nsteps; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, WAIT_BUDGET)) {
+          *abort_flag = 1;
+          atomicOr(p.status, DS_TIMEOUT);
+          break;
+        }
+        uint8_t* st = a_base + (size_t)s * 2 * A_TILE_BYTES;
+        mbar_arrive_expect_tx(&tma_full[s], 2u * A_TILE_BYTES);
+        const int32_t x = (int32_t)(kbeg + (int64_t)it * TC_BK);
+        const int32_t y = (int32_t)m0;
+        tma_load_2d(st, &map_hi, x, y, &tma_full[s]);
+        tma_load_2d(st + A_TILE_BYTES, &map_lo, x, y, &tma_full[s]);
+        issued_upto = it + 1;
+      }
+      // drain: every issued copy must have landed before the CTA may exit
+      for (int it = issued_upto - S > 0 ? issued_upto - S : 0; it < issued_upto; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        long long t0 = clock64();
+        while (!mbar_try_wait(&tma_full[s], ph) && clock64() - t0 < WAIT_BUDGET) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(TC_BM, p.n_pad);
+      bool ok = mbar_wait(b_ready, 0, abort_flag, WAIT_BUDGET);
+      for (int r = 0; ok && r < nruns; ++r) {
+        const int b = r & 1;
+        // buffer b was last used by run r - 2: wait until the epilogue read it
+        if (r >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)((r >> 1) - 1) & 1u, abort_flag,
+                                 WAIT_BUDGET)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc_hh = tmem + (uint32_t)(2 * b * p.acc_cols);
+        const uint32_t acc_cr = acc_hh + (uint32_t)p.acc_cols;
+        for (int sp = 0; sp < spr; ++sp) {
+          const int it = r * spr + sp;
+          const int s = it % S;
+          const uint32_t ph = (uint32_t)(it / S) & 1u;
+          if (!mbar_wait(&tma_full[s], ph, abort_flag, WAIT_BUDGET)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_hi = smem_u32(a_base + (size_t)s * 2 * A_TILE_BYTES);
+          const uint32_t a_lo = a_hi + A_TILE_BYTES;
+          const uint32_t b_hi = smem_u32(b_base) + (uint32_t)sp * 2u * bblk;
+          const uint32_t b_lo = b_hi + bblk;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk) {
+            const uint32_t koff = kk * 32;  // 16 bf16 = 32 bytes along K
+            const uint64_t dah = desc_sw128_kmajor(a_hi + koff);
+            const uint64_t dal = desc_sw128_kmajor(a_lo + koff);
+            const uint64_t dbh = desc_sw128_kmajor(b_hi + koff);
+            const uint64_t dbl = desc_sw128_kmajor(b_lo + koff);
+            const uint32_t first = (sp == 0 && kk == 0) ? 0u : 1u;
+            mma_bf16(acc_hh, dah, dbh, idesc, first);
+            mma_bf16(acc_cr, dah, dbl, idesc, first);
+            mma_bf16(acc_cr, dal, dbh, idesc, 1u);
+          }
+          mma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[b]);
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicOr(p.status, DS_TIMEOUT);
+      }
+      // no MMA may still be running when TMEM is freed (bounded wait)
+      mma_commit(mma_done);
+      long long t0 = clock64();
+      while (!mbar_try_wait(mma_done, 0) && clock64() - t0 < WAIT_BUDGET) {
+      }
+    }
+  } else {
+    // warps 2..5: write U_last as the B operand and the runs' weights once,
+    // then consume every run's accumulators
+    const int t = threadIdx.x - 64;
+    const KRSpec& kr = p.kr;
+    const int R = kr.R;
+    const int last = kr.n_other - 1;
+    const float* ul = kr.f[last];
+    {
+      // U_last rows kq*8 .. +7 of each 64-row k-block, columns n0 .. n0+3:
+      // two k-blocks of loads in flight at a time (128-bit when aligned)
+      const int kq = t & 7, n0 = (t >> 3) * 4;
+      const bool vec = (R & 3) == 0 && ((uintptr_t)ul & 15) == 0;
+      if (n0 < p.n_pad) {
+        for (int kb0 = 0; kb0 < spr; kb0 += 2) {
+          float v[2][4][8];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int kb = kb0 + h;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const int64_t k = (int64_t)kb * TC_BK + kq * 8 + e;
+              if (kb < spr && vec && n0 < R) {
+                const float4 x = __ldg(reinterpret_cast<const float4*>(ul + k * R + n0));
+                v[h][0][e] = x.x;
+                v[h][1][e] = x.y;
+                v[h][2][e] = x.z;
+                v[h][3][e] = x.w;
+              } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                  v[h][c][e] = (kb < spr && n0 + c < R) ? __ldg(ul + k * R + n0 + c) : 0.f;
+              }
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            if (kb0 + h < spr) {
+              uint8_t* bh = b_base + (size_t)(kb0 + h) * 2 * bblk;
+#pragma unroll
+              for (int c = 0; c < 4; ++c) store_kr_chunk(bh, bh + bblk, n0 + c, kq, v[h][c]);
+            }
+          }
+        }
+      }
+      // weights: run P = kbeg / L + r decomposes over the slower other modes;
+      // every load of every run is issued before the products are formed
+      if (t < 64) {
+        const int64_t run0 = kbeg / p.L;
+        float f[TCS_MAX_RUNS][kMaxModes - 1];
+#pragma unroll
+        for (int r = 0; r < TCS_MAX_RUNS; ++r) {
+          uint32_t idx = (uint32_t)(run0 + r);
+#pragma unroll
+          for (int q = kMaxModes - 2; q >= 0; --q) {
+            f[r][q] = 1.f;
+            if (q < last && r < nruns) {
+              const uint32_t sz = kr.size[q];
+              const uint32_t qq = idx / sz;
+              const uint32_t iq = idx - qq * sz;
+              idx = qq;
+              if (t < R) f[r][q] = __ldg(kr.f[q] + (size_t)iq * R + t);
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < TCS_MAX_RUNS; ++r) {
+          if (r < nruns) {
+            float w = t < R ? 1.f : 0.f;
+#pragma unroll
+            for (int q = 0; q < kMaxModes - 1; ++q) w *= f[r][q];
+            wts[r * 64 + t] = w;
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(b_ready);
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps: weights visible
+    }
+    const int q = warp & 3;  // TMEM lane quadrant this warp may access
+    const int64_t row = m0 + q * 32 + lane;
+    float acc[64];
+#pragma unroll
+    for (int n = 0; n < 64; ++n) acc[n] = 0.f;
+    bool ok = true;
+    for (int r = 0; r < nruns; ++r) {
+      const int b = r & 1;
+      int w_ok = 1;
+      if (lane == 0)
+        w_ok = mbar_wait(&acc_full[b], (uint32_t)(r >> 1) & 1u, abort_flag, WAIT_BUDGET) ? 1 : 0;
+      w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+      if (!w_ok) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(2 * b * p.acc_cols);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {  // columns 32h .. 32h + 31
+        if (32 * h < p.n_pad) {
+          uint32_t rh[2][16], rc[2][16];
+#pragma unroll
+          for (int g = 0; g < 2; ++g)
+            if (32 * h + 16 * g < p.n_pad) {  // warp-uniform
+              tmem_ld16_nowait(base + (uint32_t)(32 * h + 16 * g), rh[g]);
+              tmem_ld16_nowait(base + (uint32_t)(p.acc_cols + 32 * h + 16 * g), rc[g]);
+            }
+          tmem_wait_ld();
+#pragma unroll
+          for (int g = 0; g < 2; ++g)
+            if (32 * h + 16 * g < p.n_pad) {
+#pragma unroll
+              for (int i = 0; i < 16; ++i) {
+                const int n = 32 * h + 16 * g + i;
+                const float v = __uint_as_float(rh[g][i]) + __uint_as_float(rc[g][i]);
+                acc[n] = fmaf(v, wts[r * 64 + n], acc[n]);
+              }
+            }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);
+    }
+    if (row < p.rows) {
+      float* out = p.partials + (int64_t)blockIdx.x * p.rows * R + row * R;
+      if (!ok && lane == 0) atomicOr(p.status, DS_TIMEOUT);
+#pragma unroll
+      for (int n = 0; n < 64; ++n)
+        if (n < R) out[n] = ok ? acc[n] : 0.f;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, (uint32_t)(4 * p.acc_cols));
+  }
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // dependency on libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -456,6 +762,8 @@ constexpr int kTcMaxSmem = 227 * 1024;
 }  // namespace
 
 void init_tc_attributes() {
+  cudaFuncSetAttribute(mttkrp_bf16x3_runs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kTcMaxSmem);
   cudaFuncSetAttribute(mttkrp_bf16x3_kernel<true, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kTcMaxSmem);
   cudaFuncSetAttribute(mttkrp_bf16x3_kernel<false, false>,
@@ -466,12 +774,31 @@ bool tc_supported(const Unfolding& u, int R) {
   return R >= 1 && n_pad_of(R) <= 256 && u.cols < (int64_t)INT32_MAX && u.rows < INT32_MAX;
 }
 
-SplitPlan plan_tc(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
-  (void)R;
+// Run length of the prefix-scaled kernel for this unfolding and rank, or 0
+// when it does not apply.
+int tc_run_length(const Unfolding& u, int R) {
+  if (u.n_other < 1 || n_pad_of(R) > 64) return 0;
+  const int64_t L = u.other_size[u.n_other - 1];
+  if (L % TC_BK != 0 || L > TCS_MAX_L) return 0;
+  return (int)L;
+}
+
+SplitPlan plan_tc(const tsr_ctx* ctx, const Unfolding& u, int R) {
   SplitPlan p;
+  const int64_t rows = u.rows, K = u.cols;
   int64_t mt = ceil_div(rows, TC_BM);
-  int64_t steps = ceil_div(K, TC_BK);
   int64_t want = std::max<int64_t>(1, (ctx->sm_count - ctx->reserve_sms) / mt);
+  const int L = tc_run_length(u, R);
+  if (L > 0) {
+    const int64_t runs = K / L;
+    int64_t per = ceil_div(runs, std::min<int64_t>(want, runs));
+    per = std::min<int64_t>(per, TCS_MAX_RUNS);
+    p.k_per_split = per * L;
+    p.splits = (int)ceil_div(runs, per);
+    p.run_length = L;
+    return p;
+  }
+  int64_t steps = ceil_div(K, TC_BK);
   want = std::min<int64_t>(want, steps);
   int64_t steps_per = ceil_div(steps, want);
   p.k_per_split = steps_per * TC_BK;
@@ -486,6 +813,32 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
   CUtensorMap mh, ml;
   TSR_TRY(make_map(&mh, hi, u.rows, u.cols, u.ld));
   TSR_TRY(make_map(&ml, lo, u.rows, u.cols, u.ld));
+  if (plan.run_length > 0) {
+    if (plan.run_length != tc_run_length(u, kr.R) || plan.k_per_split % plan.run_length != 0 ||
+        plan.k_per_split / plan.run_length > TCS_MAX_RUNS)
+      return fail(TSR_E_INVALID_ARG, "BF16X3 MTTKRP: split plan does not match the unfolding");
+    TcsParams q;
+    q.rows = u.rows;
+    q.K = u.cols;
+    q.k_per_split = plan.k_per_split;
+    q.L = plan.run_length;
+    q.n_pad = n_pad_of(kr.R);
+    q.acc_cols = q.n_pad <= 32 ? 32 : 64;
+    q.kr = kr;
+    q.partials = partials;
+    q.status = ctx->d_status;
+    const size_t fixed = 1024 + (size_t)(q.L / TC_BK) * 2 * q.n_pad * 128 +
+                         sizeof(float) * TCS_MAX_RUNS * 64 + 8 * 64 + 16;
+    q.stages = (int)std::min<size_t>(4, (kTcMaxSmem - fixed) / (2 * A_TILE_BYTES));
+    if (q.stages < 2) return fail(TSR_E_UNSUPPORTED, "MTTKRP stage ring too large");
+    const size_t smem = fixed + (size_t)q.stages * 2 * A_TILE_BYTES;
+    dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, TC_BM));
+    if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
+    mttkrp_bf16x3_runs_kernel<<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, q);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    return TSR_OK;
+  }
   TcParams p;
   p.rows = u.rows;
   p.K = u.cols;

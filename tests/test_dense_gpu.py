@@ -80,6 +80,32 @@ def test_mttkrp_parity(orc, shape, R, precision, tol):
         assert e <= tol, (shape, R, mode, precision, e)
 
 
+# Shapes whose fastest other mode is a multiple of 64 (<= 384) take the
+# tensor-core path that scales U_last per run of KR rows; these cover run
+# lengths 64..384, ranks that are not multiples of 16, partial 128-row tiles,
+# 4-way run weights and up to 8 runs per CTA.
+RUN_SHAPES = [
+    ((130, 5, 192), 40),
+    ((70, 6, 4, 128), 17),
+    ((40, 7, 384), 64),
+    ((300, 64, 64), 16),
+    ((128, 1024, 64), 8),
+    ((33, 2, 3, 64), 1),
+]
+
+
+@pytest.mark.parametrize("shape,R", RUN_SHAPES)
+def test_mttkrp_run_scaled_path(orc, shape, R):
+    X, fs = rand_problem(shape, R, seed=hash((shape, R)) & 0xFFFF, dist="normal")
+    X64 = X.astype(np.float64)
+    f64 = [f.astype(np.float64) for f in fs]
+    for mode in range(len(shape)):
+        out = tb.mttkrp(X, fs, mode, precision="bf16x3")
+        ref = orc.mttkrp(X64, f64, mode)
+        e = rel_err(out, ref)
+        assert e <= 1e-4, (shape, R, mode, e)
+
+
 @pytest.mark.parametrize("precision,tol", [("fp32", 1e-5), ("bf16x3", 1e-4)])
 def test_mttkrp_signed_data(orc, precision, tol):
     X, fs = rand_problem((48, 40, 36), 16, seed=3, dist="normal")
