@@ -16,10 +16,6 @@ namespace tsr {
 
 namespace {
 
-__device__ __forceinline__ double sym(const double* g, int R, int a, int c) {
-  return a <= c ? g[a * R + c] : g[c * R + a];
-}
-
 // Upper triangle of U^T U accumulated into `gram` (pre-zeroed) with one FP64
 // atomic per entry per CTA. Thread (ty, tx) of a 16 x 16 grid owns entries
 // (ty + 16a, tx + 16b); rows are staged through shared memory in chunks, so a
@@ -306,83 +302,30 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
   if (last && threadIdx.x == 0) st->inner = 0.0;
 }
 
-// rows_per_cta rows of U_mode = (sum over splits of the partial MTTKRP) . G^-1.
-// Shared: G^-1 (R x R) and M (rows_per_cta x R), both FP64.
-__global__ void __launch_bounds__(256)
-solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
-             int rows_per_cta, float* __restrict__ U, int last) {
-  extern __shared__ double sh[];
-  AlsState* st = b.state;
-  if (st->done) return;
-  const int RR = R * R;
-  double* Gi = sh;
-  double* Ms = sh + RR;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
-  const int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
-#pragma unroll 8
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
-  const int64_t pstride = rows * R;
-  // every thread sums a strided subset of the split partials of one element
-  // (16 loads in flight per batch), then the groups combine in shared memory
-  const int ne = nr * R;
-  const int full = rows_per_cta * R;  // the host sized `red` from this
-  const int groups = full >= (int)blockDim.x ? 1 : (int)blockDim.x / full;
-  double* red = Ms + rows_per_cta * R;  // [groups][ne]
-  for (int t = threadIdx.x; t < ne * groups; t += blockDim.x) {
-    const int e = t % ne, g = t / ne;
-    const float* p = partials + r0 * R + e;
-    double s = 0.0;
-    int q = g;
-    for (; q + 15 * groups < splits; q += 16 * groups) {
-      float v[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) v[u] = __ldg(p + (int64_t)(q + u * groups) * pstride);
-#pragma unroll
-      for (int u = 0; u < 16; ++u) s += (double)v[u];
-    }
-    for (; q < splits; q += groups) s += (double)__ldg(p + (int64_t)q * pstride);
-    red[g * ne + e] = s;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-    double s = 0.0;
-    for (int g = 0; g < groups; ++g) s += red[g * ne + e];
-    Ms[e] = s;
-  }
-  __syncthreads();
-  double ip = 0.0;
-  for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
-    const int i = e / R, c = e % R;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four chains for ILP
-    int k = 0;
-    for (; k + 4 <= R; k += 4) {
-      s0 += Ms[i * R + k] * Gi[k * R + c];
-      s1 += Ms[i * R + k + 1] * Gi[(k + 1) * R + c];
-      s2 += Ms[i * R + k + 2] * Gi[(k + 2) * R + c];
-      s3 += Ms[i * R + k + 3] * Gi[(k + 3) * R + c];
-    }
-    for (; k < R; ++k) s0 += Ms[i * R + k] * Gi[k * R + c];
-    const double s = (s0 + s1) + (s2 + s3);
-    const float v = (float)s;
-    U[(r0 + i) * R + c] = v;
-    ip += Ms[e] * (double)v;
-  }
-  if (last) {
-    for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&st->inner, ip);
-  }
+// Thread groups per element in the split sums of a chunk of `full` outputs:
+// 256 threads cover full / 4 float4 columns (R a multiple of 4) or `full`
+// scalars, the rest of the threads take interleaved subsets of the splits.
+__host__ __device__ inline int solve_groups(int full, int R) {
+  const int cols = (R & 3) == 0 ? full / 4 : full;
+  return cols >= 256 ? 1 : 256 / cols;
 }
 
-__global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
+// fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
+// core.rs:142-166), run by one whole CTA once the last mode's Gram and <X, Xhat>
+// are complete. Those two were accumulated by atomics of other CTAs of the
+// same grid, so they are read through L2 (ld.global.cg).
+__device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
   AlsState* st = b.state;
-  if (st->done) return;
   const int RR = R * R;
   const int last = ndim - 1;
   const double* H = b.hadam + (int64_t)last * RR;
   const double* g = b.grams + (int64_t)last * RR;
   double s = 0.0;
 #pragma unroll 8
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) s += H[e] * sym(g, R, e / R, e % R);
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
+    const int a = e / R, c = e % R;
+    s += H[e] * __ldcg(g + (a <= c ? a * R + c : c * R + a));
+  }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   __shared__ double ws[32];
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
@@ -390,13 +333,11 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
   if (threadIdx.x != 0) return;
   double rn = 0.0;
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) rn += ws[w];
-  // helpers.rs:513-530
   const double xn = st->xnorm_sq;
-  const double err_sq = xn + rn - 2.0 * st->inner;
+  const double err_sq = xn + rn - 2.0 * __ldcg(&st->inner);
   const double err = sqrt(fmax(err_sq, 0.0));
   double fit = 1.0 - err / sqrt(xn);
   fit = fmin(fmax(fit, 0.0), 1.0);
-  // core.rs:142-166
   const int iter = st->iter;
   st->fit = fit;
   b.history[iter] = fit;
@@ -417,10 +358,174 @@ __global__ void fit_kernel(AlsBuffers b, int ndim, int R, double tol) {
   st->prev_fit = fit;
 }
 
+// U_mode = (sum over splits of the partial MTTKRP) . G^-1, then the Gram of
+// the new factor, U^T U (upper triangle, FP64, into `gram`, which the inverse
+// kernel of this mode zeroed), and for the last mode <M, U> = <X, Xhat> and,
+// in the CTA that finishes last, the fit and the stopping rules.
+//
+// Each CTA walks chunks of rpc rows (grid-strided): the split partials of a
+// chunk are summed in FP64 into shared memory (float4 loads, 16 in flight per
+// thread, the threads beyond one per column group taking interleaved subsets
+// of the splits), multiplied by G^-1 (shared), rounded to fp32 for U, and the
+// rounded rows are added into the thread's RB x RB block of the Gram (thread
+// (ty, tx) owns entries (ty + 16a, tx + 16b), as in gram_kernel); one FP64
+// atomic per owned upper entry at the end. Products of fp32 values are exact
+// in FP64, so the Gram equals gram_kernel's up to the order of the sums.
+template <int RB>
+__global__ void __launch_bounds__(256)
+solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
+             int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
+             double tol) {
+  extern __shared__ double sh[];
+  __shared__ int s_last;
+  AlsState* st = b.state;
+  if (st->done) return;
+  const int RR = R * R;
+  double* Gi = sh;               // R x R
+  double* Ms = Gi + RR;          // rpc x R  (FP64 MTTKRP rows)
+  double* Us = Ms + rpc * R;     // rpc x R  (the fp32 factor rows, widened)
+  double* red = Us + rpc * R;    // [groups][rpc x R]
+#pragma unroll 8
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
+  const int64_t pstride = rows * R;
+  const int full = rpc * R;
+  const int groups = solve_groups(full, R);
+  // float4 loads of the partials when rows of R floats keep 16-byte alignment
+  const bool vec = (R & 3) == 0 && ((uintptr_t)partials & 15) == 0;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[RB][RB];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = 0.0;
+  double ip = 0.0;
+  for (int64_t r0 = (int64_t)blockIdx.x * rpc; r0 < rows; r0 += (int64_t)gridDim.x * rpc) {
+    const int nr = (int)(rows - r0 < rpc ? rows - r0 : rpc);
+    const int ne = nr * R;
+    __syncthreads();  // G^-1 staged; the previous chunk's Ms / Us are consumed
+    if (vec) {
+      const int ne4 = ne >> 2;
+      const int64_t pstride4 = pstride >> 2;
+      for (int t = threadIdx.x; t < ne4 * groups; t += blockDim.x) {
+        const int e4 = t % ne4, g = t / ne4;
+        const float4* p = reinterpret_cast<const float4*>(partials + r0 * R) + e4;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int q = g;
+        for (; q + 15 * groups < splits; q += 16 * groups) {
+          float4 v[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) v[u] = __ldg(p + (int64_t)(q + u * groups) * pstride4);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            s0 += (double)v[u].x;
+            s1 += (double)v[u].y;
+            s2 += (double)v[u].z;
+            s3 += (double)v[u].w;
+          }
+        }
+        for (; q < splits; q += groups) {
+          const float4 v = __ldg(p + (int64_t)q * pstride4);
+          s0 += (double)v.x;
+          s1 += (double)v.y;
+          s2 += (double)v.z;
+          s3 += (double)v.w;
+        }
+        double* r = red + g * ne + 4 * e4;
+        r[0] = s0;
+        r[1] = s1;
+        r[2] = s2;
+        r[3] = s3;
+      }
+    } else {
+      for (int t = threadIdx.x; t < ne * groups; t += blockDim.x) {
+        const int e = t % ne, g = t / ne;
+        const float* p = partials + r0 * R + e;
+        double s = 0.0;
+        int q = g;
+        for (; q + 15 * groups < splits; q += 16 * groups) {
+          float v[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) v[u] = __ldg(p + (int64_t)(q + u * groups) * pstride);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) s += (double)v[u];
+        }
+        for (; q < splits; q += groups) s += (double)__ldg(p + (int64_t)q * pstride);
+        red[g * ne + e] = s;
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+      double s = 0.0;
+      for (int g = 0; g < groups; ++g) s += red[g * ne + e];
+      Ms[e] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+      const int i = e / R, c = e % R;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four chains for ILP
+      int k = 0;
+      for (; k + 4 <= R; k += 4) {
+        s0 += Ms[i * R + k] * Gi[k * R + c];
+        s1 += Ms[i * R + k + 1] * Gi[(k + 1) * R + c];
+        s2 += Ms[i * R + k + 2] * Gi[(k + 2) * R + c];
+        s3 += Ms[i * R + k + 3] * Gi[(k + 3) * R + c];
+      }
+      for (; k < R; ++k) s0 += Ms[i * R + k] * Gi[k * R + c];
+      const float v = (float)((s0 + s1) + (s2 + s3));
+      U[(r0 + i) * R + c] = v;
+      Us[e] = (double)v;
+      ip += Ms[e] * (double)v;
+    }
+    __syncthreads();
+    for (int i = 0; i < nr; ++i) {
+      double x[RB], y[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) {
+        const int a = ty + 16 * ai;
+        x[ai] = a < R ? Us[i * R + a] : 0.0;
+      }
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) {
+        const int c = tx + 16 * bj;
+        y[bj] = c < R ? Us[i * R + c] : 0.0;
+      }
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = fma(x[ai], y[bj], acc[ai][bj]);
+    }
+  }
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int a = ty + 16 * ai, c = tx + 16 * bj;
+      if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
+    }
+  if (!last) return;
+  for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&st->inner, ip);
+  // the CTA that arrives last sees every other CTA's Gram and <M, U> atomics
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) st->ticket = 0;
+  fit_block(b, ndim, R, tol);
+}
+
 }  // namespace
 
 void init_als_attributes() {
-  cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(solve_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int R,
@@ -472,23 +577,33 @@ int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int
 }
 
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
-                 int splits, int64_t rows, int R, float* U, bool last) {
-  // enough CTAs to spread the split-K partial reads over the SMs
-  const int rpc =
-      (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 2 * ctx->sm_count)));
-  const int ne = rpc * R;
-  const int groups = ne >= 256 ? 1 : 256 / ne;
-  const size_t smem = (size_t)(R * R + rpc * R + (size_t)groups * ne) * sizeof(double);
+                 int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
+                 double tol) {
+  if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
+  // about 64 row chunks (one per CTA) for small modes, so that the Gram
+  // atomics stay few; 16-row chunks grid-strided over at most 8 CTAs per SM
+  // for large ones
+  const int rpc = (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 64)));
+  const unsigned grid =
+      (unsigned)std::min<int64_t>(ceil_div(rows, rpc), 8 * (int64_t)ctx->sm_count);
+  const int full = rpc * R;
+  const int groups = solve_groups(full, R);
+  const size_t smem = (size_t)(R * R + 2 * full + (size_t)groups * full) * sizeof(double);
   if (smem > 200 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
-  solve_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, s>>>(b, partials, splits, rows, R,
-                                                                rpc, U, last ? 1 : 0);
-  ctx->launches++;
-  TSR_CUDA(cudaGetLastError());
-  return TSR_OK;
-}
-
-int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol) {
-  fit_kernel<<<1, 256, 0, s>>>(b, ndim, R, tol);
+  const int lst = last ? 1 : 0;
+#define TSR_SOLVE(RB)                                                                       \
+  solve_kernel<RB><<<grid, 256, smem, s>>>(b, partials, splits, rows, R, rpc, U, gram, lst, \
+                                           ndim, tol)
+  switch ((R + 15) / 16) {
+    case 1: TSR_SOLVE(1); break;
+    case 2: TSR_SOLVE(2); break;
+    case 3: TSR_SOLVE(3); break;
+    case 4: TSR_SOLVE(4); break;
+    case 5: TSR_SOLVE(5); break;
+    case 6: TSR_SOLVE(6); break;
+    default: TSR_SOLVE(7); break;
+  }
+#undef TSR_SOLVE
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

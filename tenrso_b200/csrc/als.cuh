@@ -19,7 +19,8 @@ struct AlsState {
   int done;             // stop flag: converged, oscillation or error
   unsigned status;      // DevStatus bits
   int ridge_used;
-  int pad[2];
+  unsigned ticket;      // CTAs of the last mode's solve that have finished
+  int pad;
 };
 
 struct AlsBuffers {
@@ -70,10 +71,12 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 // zeroing of gram[mode] (and, when `last`, state->inner) before the solve.
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
                 float ridge_eps, bool last);
-// U_mode = (sum of split partials) . G^{-1}; `last` accumulates <M, U>.
+// U_mode = (sum of split partials) . G^{-1} and its Gram U^T U added into
+// `gram` (zeroed by this mode's launch_chol); `last` also accumulates <M, U>
+// and applies the fit and the rules of cp/core.rs:142-166 in the CTA that
+// finishes last.
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
-                 int splits, int64_t rows, int R, float* U, bool last);
-// fit, fit_history, oscillation and convergence rules of cp/core.rs:142-166.
-int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol);
+                 int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
+                 double tol);
 
 }  // namespace tsr

@@ -205,9 +205,10 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
 // ---------------------------------------------------------------------------
 // CP-ALS driver (cp/core.rs:59-182) on a device-resident tensor.
 //
-// One ALS sweep runs on two streams so that the FP64 work overlaps the
-// MTTKRPs: the main stream carries MTTKRP_n -> solve_n, the aux stream
-// gram_{n-1} -> inverse_n (concurrent with MTTKRP_n) and the fit. The sweep is
+// One ALS sweep runs on two streams so that the FP64 inverse overlaps the
+// MTTKRP: the main stream carries MTTKRP_n -> solve_n (which also forms the
+// Gram of the new U_n and, for the last mode, the fit), the aux stream
+// inverse_n, which starts when solve_{n-1} has finished. The sweep is
 // captured once into a CUDA graph and replayed max_iters times; every kernel
 // returns at entry once the device-side stop flag is set, which reproduces the
 // reference's early exits without host round trips.
@@ -244,15 +245,13 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
       TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
     TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
     TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
-                         const_cast<float*>(a.ft.ptr[n]), last));
-    TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
-    TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
-    TSR_TRY(launch_gram(ctx, B, a.ft.ptr[n], a.shape[n], a.R,
-                        a.b.grams + (size_t)n * a.R * a.R, false));
+                         const_cast<float*>(a.ft.ptr[n]), a.b.grams + (size_t)n * a.R * a.R,
+                         last, a.ndim, a.tol));
+    if (!last) {  // the next inverse needs this mode's Gram
+      TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
+      TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
+    }
   }
-  TSR_TRY(launch_fit(ctx, B, a.b, a.ndim, a.R, a.tol));
-  TSR_CUDA(cudaEventRecord(ctx->ev[23], B));
-  TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[23], 0));
   return TSR_OK;
 }
 

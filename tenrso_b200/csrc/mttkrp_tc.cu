@@ -425,6 +425,7 @@ struct TcsParams {
   int64_t rows;
   int64_t K;
   int64_t k_per_split;  // a whole number of runs
+  int runs_per_split;   // k_per_split / L
   int L;                // run length, multiple of 64
   int n_pad;            // R rounded up to 16 (<= 64)
   int acc_cols;         // TMEM columns per accumulator (power of two >= max(n_pad, 32))
@@ -580,6 +581,45 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
     const int last = kr.n_other - 1;
     const float* ul = kr.f[last];
     {
+      // Every global load of the setup waits behind the TMA ring fill of all
+      // CTAs, so the loads are grouped into as few round trips as possible:
+      // the run weights' factor rows are issued first, together with the
+      // first U_last batch, and multiplied after the B operand is written.
+      //
+      // Weights: thread t covers runs r = (t >> 4) + 8j (j < 2) and columns
+      // c0 .. c0+3. Run P = run0 + r of this split decomposes mixed-radix
+      // over the slower other modes (q = last - 1 fastest), and
+      // w_P = prod_q U_q[i_q(P)] (columns >= R get weight 0).
+      const int c0 = (t & 15) * 4;
+      bool wvec = (R & 3) == 0;
+#pragma unroll
+      for (int q = 0; q < kMaxModes - 1; ++q)
+        if (q < last) wvec = wvec && ((uintptr_t)kr.f[q] & 15) == 0;
+      float4 wf[2][kMaxModes - 1];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int r = (t >> 4) + 8 * j;
+        uint32_t idx = (uint32_t)blockIdx.x * (uint32_t)p.runs_per_split + (uint32_t)r;
+#pragma unroll
+        for (int q = kMaxModes - 2; q >= 0; --q) {
+          wf[j][q] = make_float4(1.f, 1.f, 1.f, 1.f);
+          if (q < last && r < nruns) {
+            const uint32_t sz = kr.size[q];
+            const uint32_t qq = idx / sz;
+            const uint32_t iq = idx - qq * sz;
+            idx = qq;
+            const float* src = kr.f[q] + (size_t)iq * R;
+            if (wvec && c0 < R) {
+              wf[j][q] = __ldg(reinterpret_cast<const float4*>(src + c0));
+            } else {
+              wf[j][q].x = c0 < R ? __ldg(src + c0) : 1.f;
+              wf[j][q].y = c0 + 1 < R ? __ldg(src + c0 + 1) : 1.f;
+              wf[j][q].z = c0 + 2 < R ? __ldg(src + c0 + 2) : 1.f;
+              wf[j][q].w = c0 + 3 < R ? __ldg(src + c0 + 3) : 1.f;
+            }
+          }
+        }
+      }
       // U_last rows kq*8 .. +7 of each 64-row k-block, columns n0 .. n0+3:
       // two k-blocks of loads in flight at a time (128-bit when aligned)
       const int kq = t & 7, n0 = (t >> 3) * 4;
@@ -616,34 +656,20 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
           }
         }
       }
-      // weights: run P = kbeg / L + r decomposes over the slower other modes;
-      // every load of every run is issued before the products are formed
-      if (t < 64) {
-        const int64_t run0 = kbeg / p.L;
-        float f[TCS_MAX_RUNS][kMaxModes - 1];
 #pragma unroll
-        for (int r = 0; r < TCS_MAX_RUNS; ++r) {
-          uint32_t idx = (uint32_t)(run0 + r);
+      for (int j = 0; j < 2; ++j) {
+        const int r = (t >> 4) + 8 * j;
+        if (r < nruns) {
+          float4 w = make_float4(c0 < R ? 1.f : 0.f, c0 + 1 < R ? 1.f : 0.f,
+                                 c0 + 2 < R ? 1.f : 0.f, c0 + 3 < R ? 1.f : 0.f);
 #pragma unroll
-          for (int q = kMaxModes - 2; q >= 0; --q) {
-            f[r][q] = 1.f;
-            if (q < last && r < nruns) {
-              const uint32_t sz = kr.size[q];
-              const uint32_t qq = idx / sz;
-              const uint32_t iq = idx - qq * sz;
-              idx = qq;
-              if (t < R) f[r][q] = __ldg(kr.f[q] + (size_t)iq * R + t);
-            }
+          for (int q = 0; q < kMaxModes - 1; ++q) {
+            w.x *= wf[j][q].x;
+            w.y *= wf[j][q].y;
+            w.z *= wf[j][q].z;
+            w.w *= wf[j][q].w;
           }
-        }
-#pragma unroll
-        for (int r = 0; r < TCS_MAX_RUNS; ++r) {
-          if (r < nruns) {
-            float w = t < R ? 1.f : 0.f;
-#pragma unroll
-            for (int q = 0; q < kMaxModes - 1; ++q) w *= f[r][q];
-            wts[r * 64 + t] = w;
-          }
+          *reinterpret_cast<float4*>(wts + r * 64 + c0) = w;
         }
       }
       fence_proxy_async_smem();
@@ -696,12 +722,28 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
     }
-    if (row < p.rows) {
-      float* out = p.partials + (int64_t)blockIdx.x * p.rows * R + row * R;
-      if (!ok && lane == 0) atomicOr(p.status, DS_TIMEOUT);
+    // The warp's 32 rows are contiguous in the partials (row stride R): stage
+    // them through the A ring (every copy into it was consumed by an MMA
+    // that completed before the last acc_full) and store whole rows,
+    // coalesced. Row stride 65 floats keeps both shared accesses conflict-free.
+    const int64_t row0 = m0 + q * 32;
+    if (ok) {
+      float* stg = reinterpret_cast<float*>(a_base) + q * (32 * 65);
+      fence_proxy_async_smem();
 #pragma unroll
       for (int n = 0; n < 64; ++n)
-        if (n < R) out[n] = ok ? acc[n] : 0.f;
+        if (n < R) stg[lane * 65 + n] = acc[n];
+      __syncwarp();
+      float* out0 = p.partials + (int64_t)blockIdx.x * p.rows * R + row0 * R;
+      const int nrows = (int)(p.rows - row0 < 32 ? p.rows - row0 : 32);
+      for (int i = 0; i < nrows; ++i)
+        for (int c = lane; c < R; c += 32) out0[(int64_t)i * R + c] = stg[i * 65 + c];
+    } else {
+      if (lane == 0) atomicOr(p.status, DS_TIMEOUT);
+      if (row < p.rows) {
+        float* out = p.partials + (int64_t)blockIdx.x * p.rows * R + row * R;
+        for (int n = 0; n < R; ++n) out[n] = 0.f;
+      }
     }
   }
   tc_fence_before();
@@ -821,6 +863,7 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
     q.rows = u.rows;
     q.K = u.cols;
     q.k_per_split = plan.k_per_split;
+    q.runs_per_split = (int)(plan.k_per_split / plan.run_length);
     q.L = plan.run_length;
     q.n_pad = n_pad_of(kr.R);
     q.acc_cols = q.n_pad <= 32 ? 32 : 64;
