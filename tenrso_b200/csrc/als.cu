@@ -105,28 +105,58 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
 // corner 1 / p without special cases; with p <= 1 the +-1 terms do not cancel.
 // After steps 0..k-1 the matrix is symmetric within the processed and within
 // the unprocessed indices and antisymmetric across them, so column k is row k
-// with the sign of its processed entries flipped: each step needs only row k,
-// published by its owners into a double buffer, and one barrier.
+// with the sign of its processed entries flipped: u and w both follow from
+// row k alone.
 //
 // Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
-// (RB x RB doubles in registers). A pivot that is not positive or not finite
-// (including a non-positive diagonal) reports "not SPD"; every thread reads
-// the same pivot, so the decision is uniform.
+// (RB x RB doubles in registers). The 16 owners of row k + 1 (one half-warp)
+// update that row first, form u and w of step k + 1 from it and publish them
+// into a double buffer, so a step costs every other thread 2 RB shared loads
+// and RB^2 FMAs, and one barrier. A pivot that is not positive, not finite or
+// below 1e-290 (a non-positive diagonal included) sets the "not SPD" flag,
+// read once after the last step.
 template <int RB>
 struct GjShared {
-  double row[2][16 * RB];  // pivot row of the current step (double buffered)
-  double dsc[16 * RB];     // the diagonal scaling 1 / sqrt(G_ii)
+  double u[2][16 * RB];  // pivot column of the step, u_k = p - 1 (double buffered)
+  double w[2][16 * RB];  // pivot row of the step over p, w_k = (p + 1) / p
+  double dsc[16 * RB];   // the diagonal scaling 1 / sqrt(G_ii)
   double scale;
+  int bad;
 };
 
-// 1/p by Newton-Raphson refinement x <- x (2 - p x) of a single-precision
-// seed (two steps: about 23 -> 46 -> 92 correct bits before FP64 rounding).
-// Called for positive pivots inside float's normal range.
+// 1/p by two Newton-Raphson steps x <- x (2 - p x) from the hardware
+// approximation (rcp.approx.ftz.f64, about 20 correct bits -> 40 -> 80,
+// i.e. FP64 rounding). Called for p in [1e-290, 1].
 __device__ __forceinline__ double recip_nr(double p) {
-  double x = (double)(1.0f / (float)p);
+  double x;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(p));
   x = x * fma(-p, x, 2.0);
   x = x * fma(-p, x, 2.0);
   return x;
+}
+
+// Called by the half-warp that owns row k (ty == k & 15), `row` holding its
+// step-k values A_kj for j = tx + 16 bj: publishes u and w of step k.
+template <int RB>
+__device__ __forceinline__ void gj_publish(const double (&row)[RB], int k, int tx, int buf,
+                                           GjShared<RB>& sh) {
+  const unsigned mask = 0xFFFFu << (threadIdx.x & 16);
+  const int kb = k >> 4;
+  double mine = row[0];
+#pragma unroll
+  for (int bj = 1; bj < RB; ++bj)
+    if (bj == kb) mine = row[bj];
+  const double p = __shfl_sync(mask, mine, k & 15, 16);  // A_kk
+  const bool good = p >= 1e-290 && isfinite(p);
+  if (!good && tx == 0) sh.bad = 1;
+  const double inv = recip_nr(good ? p : 1.0);
+#pragma unroll
+  for (int bj = 0; bj < RB; ++bj) {
+    const int j = tx + 16 * bj;
+    const double r = row[bj];
+    sh.w[buf][j] = (j == k ? p + 1.0 : r) * inv;
+    sh.u[buf][j] = j == k ? p - 1.0 : (j < k ? -r : r);
+  }
 }
 
 template <int RB>
@@ -135,6 +165,7 @@ __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   // diagonal scaling (a non-positive diagonal scales its row to zero, whose
   // pivot then reports "not SPD")
+  if (threadIdx.x == 0) sh.bad = 0;
 #pragma unroll
   for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
@@ -153,44 +184,42 @@ __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
   for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
     for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
-  if (ty == 0) {
-#pragma unroll
-    for (int bj = 0; bj < RB; ++bj) sh.row[0][tx + 16 * bj] = a[0][bj];
-  }
+  if (ty == 0) gj_publish<RB>(a[0], 0, tx, 0, sh);
   __syncthreads();
 #pragma unroll 1
   for (int k = 0; k < N; ++k) {
     const int buf = k & 1;
-    const double p = sh.row[buf][k];
-    if (!(p > 0.0) || !isfinite(p)) return false;
-    const double inv = p > 1e-30 ? recip_nr(p) : 1.0 / p;
     double u[RB], w[RB];
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai) {
-      const int i = ty + 16 * ai;
-      const double r = sh.row[buf][i];
-      u[ai] = i == k ? p - 1.0 : (i < k ? -r : r);
-    }
+    for (int ai = 0; ai < RB; ++ai) u[ai] = sh.u[buf][ty + 16 * ai];
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) {
-      const int j = tx + 16 * bj;
-      const double r = sh.row[buf][j];
-      w[bj] = (j == k ? p + 1.0 : r) * inv;
+    for (int bj = 0; bj < RB; ++bj) w[bj] = sh.w[buf][tx + 16 * bj];
+    const int k1 = k + 1;
+    if (k1 < N && ty == (k1 & 15)) {
+      // row k + 1 first: its step-(k+1) u and w are the critical path. The
+      // row is picked by selects (static register indices only).
+      const int kb1 = k1 >> 4;
+      double row[RB], uk = u[0];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) row[bj] = a[0][bj];
+#pragma unroll
+      for (int ai = 1; ai < RB; ++ai) {
+        const bool sel = ai == kb1;
+        uk = sel ? u[ai] : uk;
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) row[bj] = sel ? a[ai][bj] : row[bj];
+      }
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) row[bj] = fma(-uk, w[bj], row[bj]);
+      gj_publish<RB>(row, k1, tx, buf ^ 1, sh);
     }
 #pragma unroll
     for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) a[ai][bj] = fma(-u[ai], w[bj], a[ai][bj]);
-    if (k + 1 < N) {
-#pragma unroll
-      for (int ai = 0; ai < RB; ++ai)
-        if (ty + 16 * ai == k + 1) {
-#pragma unroll
-          for (int bj = 0; bj < RB; ++bj) sh.row[buf ^ 1][tx + 16 * bj] = a[ai][bj];
-        }
-    }
     __syncthreads();
   }
+  if (sh.bad) return false;
   // G^-1 = D G'^-1 D
 #pragma unroll
   for (int ai = 0; ai < RB; ++ai)
