@@ -392,6 +392,10 @@ __device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
 // kernel of this mode zeroed), and for the last mode <M, U> = <X, Xhat> and,
 // in the CTA that finishes last, the fit and the stopping rules.
 //
+// Launched with programmatic dependent launch after the MTTKRP: G^-1 (from
+// the inverse kernel, a full dependency) is staged before the wait for the
+// MTTKRP grid.
+//
 // Each CTA walks chunks of rpc rows (grid-strided): the split partials of a
 // chunk are summed in FP64 into shared memory (float4 loads, 16 in flight per
 // thread, the threads beyond one per column group taking interleaved subsets
@@ -407,6 +411,7 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
              double tol) {
   extern __shared__ double sh[];
   __shared__ int s_last;
+  if (threadIdx.x == 0) grid_dep_trigger();
   AlsState* st = b.state;
   if (st->done) return;
   const int RR = R * R;
@@ -416,6 +421,8 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
   double* red = Us + rpc * R;    // [groups][rpc x R]
 #pragma unroll 8
   for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
+  // the partials come from the MTTKRP that precedes this kernel in its stream
+  grid_dep_wait();
   const int64_t pstride = rows * R;
   const int full = rpc * R;
   const int groups = solve_groups(full, R);
@@ -620,9 +627,9 @@ int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float*
   const size_t smem = (size_t)(R * R + 2 * full + (size_t)groups * full) * sizeof(double);
   if (smem > 200 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const int lst = last ? 1 : 0;
-#define TSR_SOLVE(RB)                                                                       \
-  solve_kernel<RB><<<grid, 256, smem, s>>>(b, partials, splits, rows, R, rpc, U, gram, lst, \
-                                           ndim, tol)
+#define TSR_SOLVE(RB)                                                                    \
+  TSR_CUDA(launch_pdl(solve_kernel<RB>, dim3(grid), dim3(256), smem, s, b, partials, splits, \
+                      rows, R, rpc, U, gram, lst, ndim, tol))
   switch ((R + 15) / 16) {
     case 1: TSR_SOLVE(1); break;
     case 2: TSR_SOLVE(2); break;

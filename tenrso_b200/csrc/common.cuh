@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/tenrso_b200.h"
@@ -109,6 +110,34 @@ int reset_status(tsr_ctx* ctx);
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+// Programmatic dependent launch. A kernel launched with launch_pdl may start
+// while the previous kernel of its stream is still running, once every CTA of
+// that kernel has called grid_dep_trigger() or exited; it must call
+// grid_dep_wait() before it reads anything the previous kernel writes or
+// writes anything that kernel reads (the wait returns once the previous grid
+// has completed and its memory is visible; without a programmatic
+// predecessor it returns at once). Only work on data produced before the
+// previous kernel may precede the wait.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Shape bookkeeping for a dense N-way tensor and one of its unfoldings.
 constexpr int kMaxModes = 8;

@@ -26,6 +26,10 @@ struct ModeOperand {
   const float* f32 = nullptr;
   const __nv_bfloat16* hi = nullptr;
   const __nv_bfloat16* lo = nullptr;
+  // written before any kernel that precedes the MTTKRP in its stream (e.g.
+  // prepared before a captured sweep): the MTTKRP may stream it before its
+  // programmatic-launch wait
+  bool resident = false;
 };
 // Bytes of the two buffers prepare_mode_into needs (0 = not needed).
 void mode_operand_bytes(const Unfolding& u, int precision, size_t* a_bytes, size_t* b_bytes);

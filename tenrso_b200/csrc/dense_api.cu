@@ -176,7 +176,7 @@ int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& 
   void* p;
   TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * partial_floats(plan, op.u.rows, R), &p));
   if (tc)
-    TSR_TRY(launch_mttkrp_tc(ctx, op.hi, op.lo, op.u, kr, plan, (float*)p));
+    TSR_TRY(launch_mttkrp_tc(ctx, op.hi, op.lo, op.u, kr, plan, (float*)p, op.resident));
   else
     TSR_TRY(launch_mttkrp_simt(ctx, op.f32, op.u, kr, plan, (float*)p));
   *partials = (float*)p;
@@ -332,6 +332,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
       SplitPlan p = tc ? plan_tc(ctx, ops[m].u, R)
                        : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
       pmax = std::max(pmax, partial_floats(p, ops[m].u.rows, R));
+      ops[m].resident = true;  // prepared here, before the sweep is enqueued
       a.op_ptrs[3 * m] = ops[m].f32;
       a.op_ptrs[3 * m + 1] = ops[m].hi;
       a.op_ptrs[3 * m + 2] = ops[m].lo;

@@ -27,9 +27,11 @@ int launch_mttkrp_reduce_scaled(tsr_ctx* ctx, const float* partials, int splits,
 // with row stride u.ld (a multiple of 8 elements, 16 bytes).
 bool tc_supported(const Unfolding& u, int R);
 SplitPlan plan_tc(const tsr_ctx* ctx, const Unfolding& u, int R);
+// a_resident: hi / lo were written before the kernel that precedes this
+// launch in the stream (see ModeOperand::resident).
 int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16* lo,
                      const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
-                     float* partials);
+                     float* partials, bool a_resident = false);
 
 // Materialised two-factor Khatri-Rao product (the public khatri_rao API).
 int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, int64_t J,

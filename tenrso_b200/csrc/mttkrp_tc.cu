@@ -433,8 +433,15 @@ struct TcsParams {
   KRSpec kr;
   float* partials;
   unsigned* status;
+  int a_resident;       // the unfolding may be streamed before the launch wait
 };
 
+// Launched with programmatic dependent launch: the previous kernel of the
+// stream (in a CP-ALS sweep, the solve that updated a factor) may still be
+// running at entry. The TMA producer streams the unfolding at once when it
+// is resident (written before that kernel); the epilogue warps wait for the
+// previous grid before they read any factor and before the partials (which
+// that kernel may read) are written.
 __global__ void __launch_bounds__(TC_THREADS, 1)
 mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
                           const __grid_constant__ CUtensorMap map_lo, TcsParams p) {
@@ -463,6 +470,7 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
   const int64_t kend = min(p.K, kbeg + p.k_per_split);
   const int nruns = kend > kbeg ? (int)((kend - kbeg) / p.L) : 0;
   const int nsteps = nruns * spr;
+  if (threadIdx.x == 0) grid_dep_trigger();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -491,6 +499,7 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
 
   if (warp == 0) {
     if (lane == 0) {
+      if (!p.a_resident) grid_dep_wait();
       int issued_upto = 0;
       for (int it = 0; it < nsteps; ++it) {
         const int s = it % S;
@@ -580,6 +589,7 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
     const int R = kr.R;
     const int last = kr.n_other - 1;
     const float* ul = kr.f[last];
+    grid_dep_wait();  // the factors (and the partials' readers) of the previous kernel
     {
       // Every global load of the setup waits behind the TMA ring fill of all
       // CTAs, so the loads are grouped into as few round trips as possible:
@@ -850,7 +860,7 @@ SplitPlan plan_tc(const tsr_ctx* ctx, const Unfolding& u, int R) {
 
 int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16* lo,
                      const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
-                     float* partials) {
+                     float* partials, bool a_resident) {
   if (!tc_supported(u, kr.R)) return fail(TSR_E_UNSUPPORTED, "BF16X3 MTTKRP: rank too large");
   CUtensorMap mh, ml;
   TSR_TRY(make_map(&mh, hi, u.rows, u.cols, u.ld));
@@ -877,7 +887,9 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
     const size_t smem = fixed + (size_t)q.stages * 2 * A_TILE_BYTES;
     dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, TC_BM));
     if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
-    mttkrp_bf16x3_runs_kernel<<<grid, TC_THREADS, smem, ctx->stream>>>(mh, ml, q);
+    q.a_resident = a_resident ? 1 : 0;
+    TSR_CUDA(launch_pdl(mttkrp_bf16x3_runs_kernel, grid, dim3(TC_THREADS), smem, ctx->stream, mh,
+                        ml, q));
     ctx->launches++;
     TSR_CUDA(cudaGetLastError());
     return TSR_OK;
