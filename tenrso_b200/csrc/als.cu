@@ -539,8 +539,16 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
       if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
     }
   if (!last) return;
+  // one <M, U> atomic per CTA (same-address atomics serialise at L2)
   for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(&st->inner, ip);
+  __syncthreads();  // the chunk loop's shared buffers are no longer read
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ip;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    atomicAdd(&st->inner, s);
+  }
   // the CTA that arrives last sees every other CTA's Gram and <M, U> atomics
   __threadfence();
   __syncthreads();

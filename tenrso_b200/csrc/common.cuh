@@ -106,6 +106,8 @@ int slot_get(tsr_ctx* ctx, int slot, size_t bytes, void** out);
 int pinned_get(tsr_ctx* ctx, size_t bytes, void** out);
 int check_ctx(tsr_ctx* ctx);
 int read_status(tsr_ctx* ctx, unsigned* out);  // synchronizes the stream
+// Evict L2 by reading a buffer of twice its size (clean lines only).
+int flush_l2(tsr_ctx* ctx, cudaStream_t s);
 int reset_status(tsr_ctx* ctx);
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

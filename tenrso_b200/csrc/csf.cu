@@ -1012,15 +1012,12 @@ int tsr_profile_mttkrp_csf_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp,
   TSR_TRY(check_ctx(ctx));
   void* dout;
   TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * sp->shape[mode] * rank, &dout));
-  void* flush = nullptr;
-  const size_t flush_bytes = std::max<size_t>(2 * ctx->l2_bytes, 256u << 20);
-  if (flush_l2) TSR_TRY(slot_get(ctx, SLOT_MISC3, flush_bytes, &flush));
   cudaEvent_t a, b;
   TSR_CUDA(cudaEventCreate(&a));
   TSR_CUDA(cudaEventCreate(&b));
   double total = 0.0;
   for (int i = 0; i < iters; ++i) {
-    if (flush_l2) TSR_CUDA(cudaMemsetAsync(flush, i & 0xff, flush_bytes, ctx->stream));
+    if (flush_l2) TSR_TRY(::tsr::flush_l2(ctx, ctx->stream));
     TSR_CUDA(cudaEventRecord(a, ctx->stream));
     TSR_TRY(tsr_mttkrp_csf_dev_f32(ctx, sp, d_factors, rank, mode, (float*)dout));
     TSR_CUDA(cudaEventRecord(b, ctx->stream));

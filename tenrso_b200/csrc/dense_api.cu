@@ -552,16 +552,13 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
   }
   ModeOperand op;
   TSR_TRY(prepare_mode(ctx, d_tensor, ndim, shape, mode, precision, 0, &op));
-  void* flush = nullptr;
-  const size_t flush_bytes = std::max<size_t>(2 * ctx->l2_bytes, 256u << 20);
-  if (flush_l2) TSR_TRY(slot_get(ctx, SLOT_MISC3, flush_bytes, &flush));
   cudaEvent_t a, b;
   TSR_CUDA(cudaEventCreate(&a));
   TSR_CUDA(cudaEventCreate(&b));
   double total = 0.0;
   int splits = 0;
   for (int i = 0; i < iters; ++i) {
-    if (flush_l2) TSR_CUDA(cudaMemsetAsync(flush, i & 0xff, flush_bytes, ctx->stream));
+    if (flush_l2) TSR_TRY(::tsr::flush_l2(ctx, ctx->stream));
     float* partials;
     TSR_CUDA(cudaEventRecord(a, ctx->stream));
     TSR_TRY(run_mttkrp_partials(ctx, op, ft, (int)rank, precision, &partials, &splits));
