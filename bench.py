@@ -460,8 +460,13 @@ def run_ours(args):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) of one launch of this kernel, mode 0, from the
+    # ncu capture summarised in profiles/mttkrp_bf16x3_256_r64_mode0.md (the
+    # three modes move the same bytes at this shape)
+    traffic = 67_302_912 + 1_162_240
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes",
+                "algorithmic_bytes": alg_bytes,
                 "kernel": "mttkrp_bf16x3_runs_kernel", "kernel_ms": kernel_ms,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
