@@ -345,6 +345,16 @@ __host__ __device__ inline int solve_groups(int full, int R) {
 // same grid, so they are read through L2 (ld.global.cg).
 __device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
   AlsState* st = b.state;
+  // the scalar state, loaded up front (the stores below could alias it)
+  double xn = 0.0, inner = 0.0, prev_fit = 0.0;
+  int iter = 0, osc = 0;
+  if (threadIdx.x == 0) {
+    xn = __ldcg(&st->xnorm_sq);
+    inner = __ldcg(&st->inner);
+    prev_fit = __ldcg(&st->prev_fit);
+    iter = __ldcg(&st->iter);
+    osc = __ldcg(&st->osc);
+  }
   const int RR = R * R;
   const int last = ndim - 1;
   const double* H = b.hadam + (int64_t)last * RR;
@@ -362,16 +372,14 @@ __device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
   if (threadIdx.x != 0) return;
   double rn = 0.0;
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) rn += ws[w];
-  const double xn = st->xnorm_sq;
-  const double err_sq = xn + rn - 2.0 * __ldcg(&st->inner);
+  const double err_sq = xn + rn - 2.0 * inner;
   const double err = sqrt(fmax(err_sq, 0.0));
   double fit = 1.0 - err / sqrt(xn);
   fit = fmin(fmax(fit, 0.0), 1.0);
-  const int iter = st->iter;
   st->fit = fit;
   b.history[iter] = fit;
-  if (iter > 0 && fit < st->prev_fit) st->osc += 1;
-  const double change = fabs(fit - st->prev_fit);
+  if (iter > 0 && fit < prev_fit) st->osc = ++osc;
+  const double change = fabs(fit - prev_fit);
   st->final_change = change;
   st->iter = iter + 1;
   if (iter > 0 && change < tol) {
@@ -379,7 +387,7 @@ __device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
     st->done = 1;
     return;
   }
-  if (st->osc > 5 && iter > 10) {
+  if (osc > 5 && iter > 10) {
     st->reason = TSR_REASON_OSCILLATION;
     st->done = 1;
     return;

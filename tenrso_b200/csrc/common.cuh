@@ -10,6 +10,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <list>
 #include <string>
 #include <utility>
 #include <vector>
@@ -94,9 +95,17 @@ struct tsr_ctx {
   cudaStream_t aux = nullptr;
   cudaEvent_t ev[24] = {};
   // cached instantiated sweep graph and the arguments it was captured with
-  cudaGraphExec_t sweep_exec = nullptr;
-  std::vector<uint8_t> sweep_key;
-  int64_t sweep_launches = 0;  // kernels per sweep graph launch
+  // Instantiated CP-ALS sweep graphs, keyed by the sweep's arguments and the
+  // number of sweeps captured; least recently used evicted beyond kMaxGraphs.
+  struct SweepGraph {
+    std::vector<uint8_t> key;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;  // kernels per graph launch
+    uint64_t last_use = 0;
+  };
+  static constexpr int kMaxGraphs = 8;
+  std::list<SweepGraph> sweep_graphs;  // stable element addresses
+  uint64_t graph_clock = 0;
 };
 
 namespace tsr {

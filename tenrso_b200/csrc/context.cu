@@ -315,7 +315,8 @@ int tsr_ctx_destroy(tsr_ctx* ctx) {
     if (b.ptr) cudaFree(b.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);
-  if (ctx->sweep_exec) cudaGraphExecDestroy(ctx->sweep_exec);
+  for (auto& g : ctx->sweep_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);

@@ -4,6 +4,7 @@
 //   tenrso_decomp::cp_als            cp/core.rs:59-182
 // Validation order and messages follow the cited lines so that a Rust shim can
 // surface them through anyhow / CpError unchanged.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -208,8 +209,8 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
 // One ALS sweep runs on two streams so that the FP64 inverse overlaps the
 // MTTKRP: the main stream carries MTTKRP_n -> solve_n (which also forms the
 // Gram of the new U_n and, for the last mode, the fit), the aux stream
-// inverse_n, which starts when solve_{n-1} has finished. The sweep is
-// captured once into a CUDA graph and replayed max_iters times; every kernel
+// inverse_n, which starts when solve_{n-1} has finished. Up to 16 sweeps are
+// captured into one CUDA graph, replayed until max_iters sweeps ran; every kernel
 // returns at entry once the device-side stop flag is set, which reproduces the
 // reference's early exits without host round trips.
 // ---------------------------------------------------------------------------
@@ -353,30 +354,60 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   const bool time_limited = time_limit_s >= 0.0;
   bool stopped_by_time = false;
   if (!time_limited && max_iters > 0) {
-    // capture (or reuse) the sweep graph and replay it max_iters times
-    std::vector<uint8_t> key((const uint8_t*)&a, (const uint8_t*)&a + sizeof(a));
-    if (!ctx->sweep_exec || key != ctx->sweep_key) {
-      if (ctx->sweep_exec) {
-        cudaGraphExecDestroy(ctx->sweep_exec);
-        ctx->sweep_exec = nullptr;
+    // Sweeps are captured kSweepsPerGraph at a time into one graph (a graph
+    // launch per sweep costs more host and front-end time than the sweep's
+    // launch gaps); whole chunks are replayed, then a graph of the remainder.
+    constexpr int kSweepsPerGraph = 16;
+    const int chunk = std::min(max_iters, kSweepsPerGraph);
+    const int n_chunks = max_iters / chunk, rem = max_iters % chunk;
+    auto graph_for = [&](int nsweeps, tsr_ctx::SweepGraph** out) -> int {
+      std::vector<uint8_t> key((const uint8_t*)&a, (const uint8_t*)&a + sizeof(a));
+      key.insert(key.end(), (const uint8_t*)&nsweeps, (const uint8_t*)&nsweeps + sizeof(nsweeps));
+      for (auto& g : ctx->sweep_graphs)
+        if (g.exec && g.key == key) {
+          g.last_use = ++ctx->graph_clock;
+          *out = &g;
+          return TSR_OK;
+        }
+      if ((int)ctx->sweep_graphs.size() >= tsr_ctx::kMaxGraphs) {
+        auto lru = std::min_element(
+            ctx->sweep_graphs.begin(), ctx->sweep_graphs.end(),
+            [](const tsr_ctx::SweepGraph& x, const tsr_ctx::SweepGraph& y) {
+              return x.last_use < y.last_use;
+            });
+        if (lru->exec) cudaGraphExecDestroy(lru->exec);
+        ctx->sweep_graphs.erase(lru);
       }
       cudaGraph_t g;
       const int64_t before = ctx->launches;
       TSR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue_sweep(ctx, a, ops);
+      int rc = TSR_OK;
+      for (int i = 0; i < nsweeps && rc == TSR_OK; ++i) rc = enqueue_sweep(ctx, a, ops);
       cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
       if (rc != TSR_OK) return rc;
       TSR_CUDA(ce);
-      ctx->sweep_launches = ctx->launches - before;
+      tsr_ctx::SweepGraph sg;
+      sg.launches = ctx->launches - before;
       ctx->launches = before;
-      cudaError_t ie = cudaGraphInstantiate(&ctx->sweep_exec, g, 0);
+      cudaError_t ie = cudaGraphInstantiate(&sg.exec, g, 0);
       cudaGraphDestroy(g);
       TSR_CUDA(ie);
-      ctx->sweep_key = key;
+      sg.key = std::move(key);
+      sg.last_use = ++ctx->graph_clock;
+      ctx->sweep_graphs.push_back(std::move(sg));
+      *out = &ctx->sweep_graphs.back();
+      return TSR_OK;
+    };
+    tsr_ctx::SweepGraph *gc = nullptr, *gr = nullptr;
+    TSR_TRY(graph_for(chunk, &gc));
+    if (rem > 0) TSR_TRY(graph_for(rem, &gr));  // evicts the least recently used, never gc
+    for (int c = 0; c < n_chunks; ++c) {
+      TSR_CUDA(cudaGraphLaunch(gc->exec, ctx->stream));
+      ctx->launches += gc->launches;
     }
-    for (int iter = 0; iter < max_iters; ++iter) {
-      TSR_CUDA(cudaGraphLaunch(ctx->sweep_exec, ctx->stream));
-      ctx->launches += ctx->sweep_launches;
+    if (rem > 0) {
+      TSR_CUDA(cudaGraphLaunch(gr->exec, ctx->stream));
+      ctx->launches += gr->launches;
     }
   } else {
     for (int iter = 0; iter < max_iters; ++iter) {
