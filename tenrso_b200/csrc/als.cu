@@ -270,15 +270,66 @@ __device__ void load_hadamard(const double* __restrict__ grams, double* __restri
     }
 }
 
+// fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
+// core.rs:142-166) of the sweep whose last solve has finished, from the
+// scalars that solve accumulated: ||X||^2 + ||Xhat||^2 - 2 <X, Xhat>. Called
+// by a whole CTA; it ends with a barrier, after which every thread may read
+// st->done.
+__device__ void fit_update(const AlsBuffers& b, double tol) {
+  AlsState* st = b.state;
+  if (threadIdx.x == 0) {
+    const double xn = __ldcg(&st->xnorm_sq);
+    const double rn = __ldcg(&st->xhat_sq);
+    const double inner = __ldcg(&st->inner);
+    const double prev_fit = __ldcg(&st->prev_fit);
+    const int iter = __ldcg(&st->iter);
+    int osc = __ldcg(&st->osc);
+    const double err_sq = xn + rn - 2.0 * inner;
+    const double err = sqrt(fmax(err_sq, 0.0));
+    double fit = 1.0 - err / sqrt(xn);
+    fit = fmin(fmax(fit, 0.0), 1.0);
+    st->fit = fit;
+    b.history[iter] = fit;
+    if (iter > 0 && fit < prev_fit) st->osc = ++osc;
+    const double change = fabs(fit - prev_fit);
+    st->final_change = change;
+    st->iter = iter + 1;
+    st->fit_pending = 0;
+    if (iter > 0 && change < tol) {
+      st->reason = TSR_REASON_FIT_TOLERANCE;
+      st->done = 1;
+    } else if (osc > 5 && iter > 10) {
+      st->reason = TSR_REASON_OSCILLATION;
+      st->done = 1;
+    } else {
+      st->prev_fit = fit;
+    }
+    __threadfence_block();
+  }
+  __syncthreads();
+}
+
+__global__ void fit_kernel(AlsBuffers b, double tol) {
+  AlsState* st = b.state;
+  if (st->done || !st->fit_pending) return;
+  fit_update(b, tol);
+}
+
 // One CTA: G = Hadamard of the other Grams and G^-1 (ridge retry, as
 // solve_least_squares does, helpers.rs:477-490); zeroes this mode's Gram
 // accumulator (and <X,Xhat> for the last mode) for the solve that follows.
 template <int RB>
 __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
-                                                   float ridge_eps, int last) {
+                                                   float ridge_eps, int last, double tol) {
   __shared__ GjShared<RB> gsh;
   AlsState* st = b.state;
   if (st->done) return;
+  if (mode == 0 && st->fit_pending) {
+    // the previous sweep's fit and stopping rules come first: a sweep that
+    // stops the run leaves the factors as they are (core.rs:142-166)
+    fit_update(b, tol);
+    if (*(volatile int*)&st->done) return;
+  }
   const int RR = R * R;
   double a[RB][RB];
   load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
@@ -328,7 +379,10 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
     }
   double* gm = b.grams + (int64_t)mode * RR;
   for (int e = threadIdx.x; e < RR; e += blockDim.x) gm[e] = 0.0;
-  if (last && threadIdx.x == 0) st->inner = 0.0;
+  if (last && threadIdx.x == 0) {
+    st->inner = 0.0;
+    st->xhat_sq = 0.0;
+  }
 }
 
 // Thread groups per element in the split sums of a chunk of `full` outputs:
@@ -339,61 +393,6 @@ __host__ __device__ inline int solve_groups(int full, int R) {
   return cols >= 256 ? 1 : 256 / cols;
 }
 
-// fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
-// core.rs:142-166), run by one whole CTA once the last mode's Gram and <X, Xhat>
-// are complete. Those two were accumulated by atomics of other CTAs of the
-// same grid, so they are read through L2 (ld.global.cg).
-__device__ void fit_block(const AlsBuffers& b, int ndim, int R, double tol) {
-  AlsState* st = b.state;
-  // the scalar state, loaded up front (the stores below could alias it)
-  double xn = 0.0, inner = 0.0, prev_fit = 0.0;
-  int iter = 0, osc = 0;
-  if (threadIdx.x == 0) {
-    xn = __ldcg(&st->xnorm_sq);
-    inner = __ldcg(&st->inner);
-    prev_fit = __ldcg(&st->prev_fit);
-    iter = __ldcg(&st->iter);
-    osc = __ldcg(&st->osc);
-  }
-  const int RR = R * R;
-  const int last = ndim - 1;
-  const double* H = b.hadam + (int64_t)last * RR;
-  const double* g = b.grams + (int64_t)last * RR;
-  double s = 0.0;
-#pragma unroll 8
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
-    const int a = e / R, c = e % R;
-    s += H[e] * __ldcg(g + (a <= c ? a * R + c : c * R + a));
-  }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  __shared__ double ws[32];
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  double rn = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) rn += ws[w];
-  const double err_sq = xn + rn - 2.0 * inner;
-  const double err = sqrt(fmax(err_sq, 0.0));
-  double fit = 1.0 - err / sqrt(xn);
-  fit = fmin(fmax(fit, 0.0), 1.0);
-  st->fit = fit;
-  b.history[iter] = fit;
-  if (iter > 0 && fit < prev_fit) st->osc = ++osc;
-  const double change = fabs(fit - prev_fit);
-  st->final_change = change;
-  st->iter = iter + 1;
-  if (iter > 0 && change < tol) {
-    st->reason = TSR_REASON_FIT_TOLERANCE;
-    st->done = 1;
-    return;
-  }
-  if (osc > 5 && iter > 10) {
-    st->reason = TSR_REASON_OSCILLATION;
-    st->done = 1;
-    return;
-  }
-  st->prev_fit = fit;
-}
 
 // U_mode = (sum over splits of the partial MTTKRP) . G^-1, then the Gram of
 // the new factor, U^T U (upper triangle, FP64, into `gram`, which the inverse
@@ -418,7 +417,6 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
              int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
              double tol) {
   extern __shared__ double sh[];
-  __shared__ int s_last;
   if (threadIdx.x == 0) grid_dep_trigger();
   AlsState* st = b.state;
   if (st->done) return;
@@ -547,25 +545,41 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
       if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
     }
   if (!last) return;
-  // one <M, U> atomic per CTA (same-address atomics serialise at L2)
-  for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
+  // ||Xhat||^2 = sum_ac H_ac (U^T U)_ac with H the Hadamard of the other
+  // Grams (this mode's inverse kernel wrote it): this CTA's share from its
+  // Gram blocks, off-diagonal entries counted twice
+  const double* H = b.hadam + (int64_t)(ndim - 1) * RR;
+  double xs = 0.0;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int a = ty + 16 * ai, c = tx + 16 * bj;
+      if (a < R && c < R && c >= a) xs += (c == a ? 1.0 : 2.0) * __ldg(H + a * R + c) * acc[ai][bj];
+    }
+  // one atomic per CTA for each sum (same-address atomics serialise at L2)
+  for (int o = 16; o > 0; o >>= 1) {
+    ip += __shfl_down_sync(0xffffffffu, ip, o);
+    xs += __shfl_down_sync(0xffffffffu, xs, o);
+  }
   __syncthreads();  // the chunk loop's shared buffers are no longer read
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ip;
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = ip;
+    red[8 + (threadIdx.x >> 5)] = xs;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    double s = 0.0, x = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      s += red[w];
+      x += red[8 + w];
+    }
     atomicAdd(&st->inner, s);
+    atomicAdd(&st->xhat_sq, x);
   }
-  // the CTA that arrives last sees every other CTA's Gram and <M, U> atomics
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (threadIdx.x == 0) st->ticket = 0;
-  fit_block(b, ndim, R, tol);
+  // the fit of this sweep is formed by the next inverse kernel (or by
+  // fit_kernel after the last sweep), once this grid's atomics are complete
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->fit_pending = 1;
 }
 
 }  // namespace
@@ -611,18 +625,25 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 }
 
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last) {
+                float ridge_eps, bool last, double tol) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const int lst = last ? 1 : 0;
   switch ((R + 15) / 16) {
-    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
-    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst); break;
+    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
   }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol) {
+  fit_kernel<<<1, 32, 0, s>>>(b, tol);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

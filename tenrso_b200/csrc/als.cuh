@@ -10,6 +10,7 @@ constexpr int kMaxRank = 112;  // two R x R FP64 matrices fit in shared memory
 struct AlsState {
   double xnorm_sq;      // ||X||^2 (FP64)
   double inner;         // <X, Xhat> accumulated by the last mode's solve
+  double xhat_sq;       // ||Xhat||^2 = sum(H_last o Gram_last), same solve
   double prev_fit;
   double fit;
   double final_change;
@@ -19,7 +20,7 @@ struct AlsState {
   int done;             // stop flag: converged, oscillation or error
   unsigned status;      // DevStatus bits
   int ridge_used;
-  unsigned ticket;      // CTAs of the last mode's solve that have finished
+  int fit_pending;      // the last solve of a sweep ran; its fit is not formed yet
   int pad;
 };
 
@@ -69,12 +70,14 @@ int launch_gram(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t rows, int 
 int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, double* out);
 // Hadamard of all Grams except `mode`, its inverse (ridge retry), and the
 // zeroing of gram[mode] (and, when `last`, state->inner) before the solve.
+// For mode 0 it first forms the fit of the previous sweep, when one is pending.
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last);
+                float ridge_eps, bool last, double tol);
+// The pending fit of the last sweep (fit, history, stopping rules).
+int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol);
 // U_mode = (sum of split partials) . G^{-1} and its Gram U^T U added into
 // `gram` (zeroed by this mode's launch_chol); `last` also accumulates <M, U>
-// and applies the fit and the rules of cp/core.rs:142-166 in the CTA that
-// finishes last.
+// and marks the sweep's fit pending.
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
                  double tol);

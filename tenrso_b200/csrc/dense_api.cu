@@ -209,7 +209,8 @@ int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
 // One ALS sweep runs on two streams so that the FP64 inverse overlaps the
 // MTTKRP: the main stream carries MTTKRP_n -> solve_n (which also forms the
 // Gram of the new U_n and, for the last mode, the fit), the aux stream
-// inverse_n, which starts when solve_{n-1} has finished. Up to 16 sweeps are
+// inverse_n, which starts when solve_{n-1} has finished (inverse_0 first
+// forms the previous sweep's fit, off the main stream). Up to 16 sweeps are
 // captured into one CUDA graph, replayed until max_iters sweeps ran; every kernel
 // returns at entry once the device-side stop flag is set, which reproduces the
 // reference's early exits without host round trips.
@@ -236,7 +237,7 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
   TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[0], 0));
   for (int n = 0; n < a.ndim; ++n) {
     const bool last = n == a.ndim - 1;
-    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last));
+    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last, a.tol));
     TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
     float* partials = a.partials;
     int splits = 1;
@@ -425,6 +426,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
       TSR_TRY(enqueue_sweep(ctx, a, ops));
     }
   }
+  if (max_iters > 0) TSR_TRY(launch_fit(ctx, ctx->stream, a.b, ndim, R, tol));
   AlsState hs;
   TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   TSR_CUDA(cudaStreamSynchronize(ctx->stream));
