@@ -11,6 +11,7 @@
 // (mathematically identical to the extra mode-0 MTTKRP of helpers.rs:558-579).
 // Grams are stored as their upper triangle (row a, column c >= a).
 #include "als.cuh"
+#include "sm100.cuh"
 
 namespace tsr {
 
@@ -416,7 +417,9 @@ __global__ void __launch_bounds__(256)
 solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
              int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
              double tol) {
-  extern __shared__ double sh[];
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t gi_bar;
+  __shared__ int gi_state;  // 0 copy in flight, 1 landed, 2 gave up
   if (threadIdx.x == 0) grid_dep_trigger();
   AlsState* st = b.state;
   if (st->done) return;
@@ -425,8 +428,30 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
   double* Ms = Gi + RR;          // rpc x R  (FP64 MTTKRP rows)
   double* Us = Ms + rpc * R;     // rpc x R  (the fp32 factor rows, widened)
   double* red = Us + rpc * R;    // [groups][rpc x R]
+  // G^-1 (a full dependency, complete at launch) comes in by bulk async
+  // copies that overlap the split sums when its size is a multiple of 16 B
+  // (R even); else by plain loads
+  const uint32_t gi_bytes = (uint32_t)RR * 8u;
+  const bool gi_bulk = (gi_bytes & 15u) == 0;
+  if (gi_bulk) {
+    if (threadIdx.x == 0) {
+      gi_state = 0;
+      sm100::mbar_init(&gi_bar, 1);
+      sm100::fence_barrier_init();
+      sm100::mbar_arrive_expect_tx(&gi_bar, gi_bytes);
+      for (uint32_t off = 0; off < gi_bytes; off += 16384u) {
+        const uint32_t n = gi_bytes - off < 16384u ? gi_bytes - off : 16384u;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(sm100::smem_u32((const char*)Gi + off)),
+            "l"((const char*)b.ginv + off), "r"(n), "r"(sm100::smem_u32(&gi_bar))
+            : "memory");
+      }
+    }
+  } else {
 #pragma unroll 8
-  for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
+    for (int e = threadIdx.x; e < RR; e += blockDim.x) Gi[e] = __ldg(b.ginv + e);
+  }
   // the partials come from the MTTKRP that precedes this kernel in its stream
   grid_dep_wait();
   const int64_t pstride = rows * R;
@@ -501,7 +526,24 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
       for (int g = 0; g < groups; ++g) s += red[g * ne + e];
       Ms[e] = s;
     }
+    if (gi_bulk && threadIdx.x == 0 && gi_state == 0) {
+      // bounded wait (~1 s); on timeout report, and let the copy land (again
+      // bounded) before the CTA may exit
+      long long t0 = clock64();
+      bool ok;
+      while (!(ok = sm100::mbar_try_wait(&gi_bar, 0)) && clock64() - t0 < (1ll << 31)) {
+      }
+      if (!ok) {
+        atomicOr(&st->status, DS_TIMEOUT);
+        st->done = 1;
+        t0 = clock64();
+        while (!sm100::mbar_try_wait(&gi_bar, 0) && clock64() - t0 < (1ll << 31)) {
+        }
+      }
+      gi_state = ok ? 1 : 2;
+    }
     __syncthreads();
+    if (gi_bulk && gi_state == 2) return;
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
       const int i = e / R, c = e % R;
       double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four chains for ILP

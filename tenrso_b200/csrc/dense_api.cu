@@ -430,6 +430,8 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   AlsState hs;
   TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (hs.status & DS_TIMEOUT)
+    return fail(TSR_E_TIMEOUT, "device wait timed out in the CP-ALS sweep");
   if (hs.status & DS_NOT_SPD)
     return fail(TSR_E_NOT_SPD,
                 "Linear algebra error: Gram matrix is not positive definite (ridge %g also "
