@@ -170,6 +170,12 @@ int launch_unfold_f32(tsr_ctx* ctx, const float* X, const int64_t* shape, const 
                       float* out);
 int launch_unfold_bf16x2(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
                          __nv_bfloat16* hi, __nv_bfloat16* lo);
+// Every unfolding of a 3-way tensor in one pass (bf16 hi/lo for all modes, or
+// fp32 for modes 1 and 2), adding ||X||^2 into *norm_sq. Needs J, K multiples
+// of 8 (unpadded rows) and I <= 65535.
+bool unfold3_supported(int ndim, const int64_t* shape);
+int launch_unfold3(tsr_ctx* ctx, const float* X, const int64_t* shape, bool bf16,
+                   void* const* hi, void* const* lo, double* norm_sq);
 
 // Raise the dynamic shared-memory limits of every kernel once per process
 // (before any stream capture).

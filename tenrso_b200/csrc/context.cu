@@ -199,6 +199,106 @@ struct StoreBF16x2 {
   }
 };
 
+// All unfoldings of a 3-way tensor X[I][J][K] (J, K multiples of 8; rows
+// unpadded) in one pass, plus ||X||^2:
+//   X_(0)[i][j*K + k], X_(1)[j][i*K + k], X_(2)[k][i*J + j]
+// as bf16 hi/lo pairs (BF16) or fp32 (modes 1 and 2 only: X is X_(0)). A CTA
+// owns a 32 (j) x 64 (k) tile of one slice i: it reads the tile once (128-bit
+// loads), writes modes 0 and 1 as 16-byte row pieces and mode 2 through a
+// shared-memory transpose, 8 consecutive j per thread. Each element's split is
+// formed once for all three copies.
+struct Unfold3Out {
+  void* hi[3];  // bf16 hi (BF16) or fp32 (else); hi[0] unused for fp32
+  void* lo[3];  // bf16 lo (BF16 only)
+};
+
+template <bool BF16>
+__device__ __forceinline__ void put8(const Unfold3Out& o, int m, int64_t off, const float (&v)[8]) {
+  if (BF16) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+      const float2 hf = __bfloat1622float2(hb);
+      const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * e] - hf.x, v[2 * e + 1] - hf.y);
+      h[e] = *reinterpret_cast<const uint32_t*>(&hb);
+      l[e] = *reinterpret_cast<const uint32_t*>(&lb);
+    }
+    *reinterpret_cast<uint4*>((__nv_bfloat16*)o.hi[m] + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>((__nv_bfloat16*)o.lo[m] + off) = make_uint4(l[0], l[1], l[2], l[3]);
+  } else {
+    float4* d = reinterpret_cast<float4*>((float*)o.hi[m] + off);
+    d[0] = make_float4(v[0], v[1], v[2], v[3]);
+    d[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(256) unfold3_kernel(const float* __restrict__ X, int I, int J,
+                                                      int K, Unfold3Out o, double* norm_sq) {
+  __shared__ float tile[64][33];  // [k][j]
+  __shared__ double ws[8];
+  const int j0 = blockIdx.x * 32, i = blockIdx.y, k0 = blockIdx.z * 64;
+  const int t = threadIdx.x;
+  const int jl = t >> 3, kl = (t & 7) * 8;
+  const int j = j0 + jl;
+  const bool in = j < J && k0 + kl < K;  // whole groups of 8 (K % 8 == 0)
+  float v[8];
+  double ss = 0.0;
+  if (in) {
+    const float4* src = reinterpret_cast<const float4*>(X + ((int64_t)i * J + j) * K + k0 + kl);
+    const float4 a = __ldg(src), b = __ldg(src + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) ss += (double)v[e] * v[e];
+    if (BF16) put8<BF16>(o, 0, ((int64_t)i * J + j) * K + k0 + kl, v);
+    put8<BF16>(o, 1, ((int64_t)j * I + i) * K + k0 + kl, v);
+  }
+#pragma unroll
+  for (int e = 0; e < 8; ++e) tile[kl + e][jl] = in ? v[e] : 0.f;
+  __syncthreads();
+  const int kk = t >> 2, jq = (t & 3) * 8;
+  if (k0 + kk < K && j0 + jq < J) {  // whole groups of 8 (J % 8 == 0)
+    float w[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) w[e] = tile[kk][jq + e];
+    put8<BF16>(o, 2, ((int64_t)(k0 + kk) * I + i) * J + j0 + jq, w);
+  }
+  for (int s = 16; s > 0; s >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, s);
+  if ((t & 31) == 0) ws[t >> 5] = ss;
+  __syncthreads();
+  if (t == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < 8; ++w) tot += ws[w];
+    atomicAdd(norm_sq, tot);
+  }
+}
+
+bool unfold3_supported(int ndim, const int64_t* shape) {
+  return ndim == 3 && shape[1] % 8 == 0 && shape[2] % 8 == 0 && shape[0] <= 65535 &&
+         shape[1] < (1 << 30) && shape[2] / 64 < 65535 && shape[0] * shape[1] * shape[2] > 0;
+}
+
+int launch_unfold3(tsr_ctx* ctx, const float* X, const int64_t* shape, bool bf16,
+                   void* const* hi, void* const* lo, double* norm_sq) {
+  if (!unfold3_supported(3, shape)) return fail(TSR_E_UNSUPPORTED, "unfold3: shape");
+  Unfold3Out o{};
+  for (int m = 0; m < 3; ++m) {
+    o.hi[m] = hi[m];
+    o.lo[m] = lo ? lo[m] : nullptr;
+  }
+  const int I = (int)shape[0], J = (int)shape[1], K = (int)shape[2];
+  dim3 grid((unsigned)ceil_div(J, 32), (unsigned)I, (unsigned)ceil_div(K, 64));
+  if (bf16)
+    unfold3_kernel<true><<<grid, 256, 0, ctx->stream>>>(X, I, J, K, o, norm_sq);
+  else
+    unfold3_kernel<false><<<grid, 256, 0, ctx->stream>>>(X, I, J, K, o, norm_sq);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
 template <class Store>
 static int launch_unfold(tsr_ctx* ctx, const float* X, const int64_t* shape, const Unfolding& u,
                          Store store) {

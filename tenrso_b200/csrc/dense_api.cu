@@ -319,6 +319,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   // in every mttkrp call, mttkrp.rs:126)
   std::vector<ModeOperand> ops(ndim);
   size_t pmax = 0;
+  const bool fused_unfold = !sp && max_iters > 0 && unfold3_supported(ndim, shape);
   if (max_iters > 0 && sp) {
     for (int m = 0; m < ndim; ++m) pmax = std::max(pmax, (size_t)shape[m] * R);
     void* pp;
@@ -328,8 +329,25 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(double) * pmax, &ap));
     a.acc64 = (double*)ap;
   } else if (max_iters > 0) {
+    // 3-way tensors: every unfolding (and ||X||^2) in one pass over X
+    void* uhi[3] = {nullptr, nullptr, nullptr};
+    void* ulo[3] = {nullptr, nullptr, nullptr};
     for (int m = 0; m < ndim; ++m) {
-      TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
+      if (fused_unfold) {
+        ops[m].u = make_unfolding(ndim, shape, m);
+        size_t ab, bb;
+        mode_operand_bytes(ops[m].u, precision, &ab, &bb);
+        if (ab) TSR_TRY(slot_get(ctx, SLOT_UNFOLD0 + m, ab, &uhi[m]));
+        if (bb) TSR_TRY(slot_get(ctx, SLOT_UNFOLD_LO + m, bb, &ulo[m]));
+        if (precision == TSR_PREC_BF16X3) {
+          ops[m].hi = (const __nv_bfloat16*)uhi[m];
+          ops[m].lo = (const __nv_bfloat16*)ulo[m];
+        } else {
+          ops[m].f32 = m == 0 ? dX : (const float*)uhi[m];
+        }
+      } else {
+        TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
+      }
       const bool tc = precision == TSR_PREC_BF16X3;
       SplitPlan p = tc ? plan_tc(ctx, ops[m].u, R)
                        : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
@@ -342,11 +360,15 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     void* pp;
     TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
     a.partials = (float*)pp;
+    if (fused_unfold)
+      TSR_TRY(launch_unfold3(ctx, dX, shape, precision == TSR_PREC_BF16X3, uhi,
+                             precision == TSR_PREC_BF16X3 ? ulo : nullptr,
+                             &a.b.state->xnorm_sq));
   }
   if (sp)  // sum of squared values, FP64, computed when the tensor was built
     TSR_CUDA(cudaMemcpyAsync(&a.b.state->xnorm_sq, &sp->norm_sq, sizeof(double),
                              cudaMemcpyHostToDevice, ctx->stream));
-  else
+  else if (!fused_unfold)
     TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, &a.b.state->xnorm_sq));
   for (int m = 0; m < ndim; ++m)
     TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,

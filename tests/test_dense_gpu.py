@@ -187,6 +187,20 @@ def test_cp_als_c1_vs_f32_reference(orc):
     assert abs(res.fit - fit_ref) <= 1e-4, (res.fit, fit_ref)
 
 
+# 3-way shapes whose middle and last sizes are multiples of 8 build every
+# unfolding (and ||X||^2) in one fused pass; these cover partial 32-wide j
+# tiles, partial 64-wide k tiles and odd first modes.
+@pytest.mark.parametrize("shape,R", [((37, 24, 40), 5), ((5, 8, 72), 3), ((70, 136, 16), 7)])
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_cp_als_fused_unfold_shapes(orc, shape, R, precision):
+    X, _ = synth.dense_lowrank(shape, R, seed=0xF0 + R, dist="normal", noise=0.01)
+    init = synth.init_factors(shape, R, 0xF0 + R)
+    _, info = orc.cp_als(X.astype(np.float64), R, 6, 0.0, [f.astype(np.float64) for f in init])
+    res = tb.cp_als(X, R, 6, 0.0, init=init, precision=precision)
+    assert res.iters == 6
+    assert abs(res.fit - info["fit"]) <= 1e-4, (shape, precision, res.fit, info["fit"])
+
+
 def test_cp_als_tolerance_stop(orc):
     X, init = _c1()
     _, info = orc.cp_als(X.astype(np.float64), 8, 50, 1e-3,
