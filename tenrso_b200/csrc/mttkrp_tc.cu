@@ -426,7 +426,7 @@ struct TcsParams {
   int64_t K;
   int64_t k_per_split;  // a whole number of runs
   int runs_per_split;   // k_per_split / L
-  int L;                // run length, multiple of 64
+  int L;                // run length, multiple of 8 (padded to 64-wide k-blocks)
   int n_pad;            // R rounded up to 16 (<= 64)
   int acc_cols;         // TMEM columns per accumulator (power of two >= max(n_pad, 32))
   int stages;
@@ -449,7 +449,7 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
   const int S = p.stages;
-  const int spr = p.L / TC_BK;                          // stages per run
+  const int spr = (p.L + TC_BK - 1) / TC_BK;            // stages per run (last one padded)
   const uint32_t bblk = (uint32_t)p.n_pad * 128u;       // one k-block of B (hi or lo)
   uint8_t* a_base = smem;
   uint8_t* b_base = smem + (size_t)S * 2 * A_TILE_BYTES;
@@ -511,10 +511,12 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
         }
         uint8_t* st = a_base + (size_t)s * 2 * A_TILE_BYTES;
         mbar_arrive_expect_tx(&tma_full[s], 2u * A_TILE_BYTES);
-        const int32_t x = (int32_t)(kbeg + (int64_t)it * TC_BK);
-        const int32_t y = (int32_t)m0;
-        tma_load_2d(st, &map_hi, x, y, &tma_full[s]);
-        tma_load_2d(st + A_TILE_BYTES, &map_lo, x, y, &tma_full[s]);
+        // [rows][runs][L] view: columns at or beyond L of a run read as zero
+        const int32_t x = (int32_t)((it % spr) * TC_BK);
+        const int32_t y = (int32_t)((int64_t)blockIdx.x * p.runs_per_split + it / spr);
+        const int32_t z = (int32_t)m0;
+        tma_load_3d(st, &map_hi, x, y, z, &tma_full[s]);
+        tma_load_3d(st + A_TILE_BYTES, &map_lo, x, y, z, &tma_full[s]);
         issued_upto = it + 1;
       }
       // drain: every issued copy must have landed before the CTA may exit
@@ -643,7 +645,10 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
               const int64_t k = (int64_t)kb * TC_BK + kq * 8 + e;
-              if (kb < spr && vec && n0 < R) {
+              if (k >= p.L) {  // padding rows of the last k-block of a run
+#pragma unroll
+                for (int c = 0; c < 4; ++c) v[h][c][e] = 0.f;
+              } else if (kb < spr && vec && n0 < R) {
                 const float4 x = __ldg(reinterpret_cast<const float4*>(ul + k * R + n0));
                 v[h][0][e] = x.x;
                 v[h][1][e] = x.y;
@@ -801,6 +806,26 @@ int make_map(CUtensorMap* map, const __nv_bfloat16* base, int64_t rows, int64_t 
   return TSR_OK;
 }
 
+// The unfolding as [rows][runs][L] (run stride L, row stride ld), 64 x 1 x 128
+// boxes: a box never crosses into the next run, and its columns at or beyond L
+// are filled with zeros. Needs L % 8 == 0 (16-byte run stride).
+int make_map_runs(CUtensorMap* map, const __nv_bfloat16* base, int64_t rows, int64_t runs,
+                  int64_t L, int64_t ld) {
+  EncodeTiledFn enc = get_encode();
+  if (!enc) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (((uintptr_t)base & 15) || (ld * 2) % 16 || (L * 2) % 16)
+    return fail(TSR_E_INVALID_ARG, "TMA operand misaligned");
+  cuuint64_t dims[3] = {(cuuint64_t)L, (cuuint64_t)runs, (cuuint64_t)rows};
+  cuuint64_t strides[2] = {(cuuint64_t)(L * 2), (cuuint64_t)(ld * 2)};
+  cuuint32_t box[3] = {(cuuint32_t)TC_BK, 1, (cuuint32_t)TC_BM};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TSR_OK;
+}
+
 int n_pad_of(int R) { return (int)round_up(R, 16); }
 
 int stages_for(int n_pad) {
@@ -831,7 +856,7 @@ bool tc_supported(const Unfolding& u, int R) {
 int tc_run_length(const Unfolding& u, int R) {
   if (u.n_other < 1 || n_pad_of(R) > 64) return 0;
   const int64_t L = u.other_size[u.n_other - 1];
-  if (L % TC_BK != 0 || L > TCS_MAX_L) return 0;
+  if (L % 8 != 0 || round_up(L, TC_BK) > TCS_MAX_L) return 0;
   return (int)L;
 }
 
@@ -863,9 +888,9 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
                      float* partials, bool a_resident) {
   if (!tc_supported(u, kr.R)) return fail(TSR_E_UNSUPPORTED, "BF16X3 MTTKRP: rank too large");
   CUtensorMap mh, ml;
-  TSR_TRY(make_map(&mh, hi, u.rows, u.cols, u.ld));
-  TSR_TRY(make_map(&ml, lo, u.rows, u.cols, u.ld));
   if (plan.run_length > 0) {
+    TSR_TRY(make_map_runs(&mh, hi, u.rows, u.cols / plan.run_length, plan.run_length, u.ld));
+    TSR_TRY(make_map_runs(&ml, lo, u.rows, u.cols / plan.run_length, plan.run_length, u.ld));
     if (plan.run_length != tc_run_length(u, kr.R) || plan.k_per_split % plan.run_length != 0 ||
         plan.k_per_split / plan.run_length > TCS_MAX_RUNS)
       return fail(TSR_E_INVALID_ARG, "BF16X3 MTTKRP: split plan does not match the unfolding");
@@ -880,7 +905,7 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
     q.kr = kr;
     q.partials = partials;
     q.status = ctx->d_status;
-    const size_t fixed = 1024 + (size_t)(q.L / TC_BK) * 2 * q.n_pad * 128 +
+    const size_t fixed = 1024 + (size_t)ceil_div(q.L, TC_BK) * 2 * q.n_pad * 128 +
                          sizeof(float) * TCS_MAX_RUNS * 64 + 8 * 64 + 16;
     q.stages = (int)std::min<size_t>(4, (kTcMaxSmem - fixed) / (2 * A_TILE_BYTES));
     if (q.stages < 2) return fail(TSR_E_UNSUPPORTED, "MTTKRP stage ring too large");
@@ -894,6 +919,8 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
     TSR_CUDA(cudaGetLastError());
     return TSR_OK;
   }
+  TSR_TRY(make_map(&mh, hi, u.rows, u.cols, u.ld));
+  TSR_TRY(make_map(&ml, lo, u.rows, u.cols, u.ld));
   TcParams p;
   p.rows = u.rows;
   p.K = u.cols;

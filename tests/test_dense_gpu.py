@@ -80,10 +80,11 @@ def test_mttkrp_parity(orc, shape, R, precision, tol):
         assert e <= tol, (shape, R, mode, precision, e)
 
 
-# Shapes whose fastest other mode is a multiple of 64 (<= 384) take the
-# tensor-core path that scales U_last per run of KR rows; these cover run
-# lengths 64..384, ranks that are not multiples of 16, partial 128-row tiles,
-# 4-way run weights and up to 8 runs per CTA.
+# Shapes whose fastest other mode is a multiple of 8 (at most 384 once padded
+# to 64) take the tensor-core path that scales U_last per run of KR rows;
+# these cover run lengths 8..384 (whole and zero-padded 64-wide k-blocks),
+# ranks that are not multiples of 16, partial 128-row tiles, 4-way run weights
+# and up to 16 runs per CTA.
 RUN_SHAPES = [
     ((130, 5, 192), 40),
     ((70, 6, 4, 128), 17),
@@ -91,6 +92,10 @@ RUN_SHAPES = [
     ((300, 64, 64), 16),
     ((128, 1024, 64), 8),
     ((33, 2, 3, 64), 1),
+    ((70, 6, 48), 17),
+    ((16, 12, 8, 48), 32),
+    ((50, 9, 104), 20),
+    ((24, 40, 8), 5),
 ]
 
 
