@@ -360,19 +360,29 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     void* pp;
     TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
     a.partials = (float*)pp;
-    if (fused_unfold)
+    if (fused_unfold) {
+      // the initial Grams run on the aux stream beside the unfold pass
+      TSR_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+      TSR_CUDA(cudaStreamWaitEvent(ctx->aux, ctx->ev[0], 0));
+      for (int m = 0; m < ndim; ++m)
+        TSR_TRY(launch_gram(ctx, ctx->aux, a.ft.ptr[m], shape[m], R,
+                            a.b.grams + (size_t)m * R * R, false));
+      TSR_CUDA(cudaEventRecord(ctx->ev[1], ctx->aux));
       TSR_TRY(launch_unfold3(ctx, dX, shape, precision == TSR_PREC_BF16X3, uhi,
                              precision == TSR_PREC_BF16X3 ? ulo : nullptr,
                              &a.b.state->xnorm_sq));
+      TSR_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev[1], 0));
+    }
   }
   if (sp)  // sum of squared values, FP64, computed when the tensor was built
     TSR_CUDA(cudaMemcpyAsync(&a.b.state->xnorm_sq, &sp->norm_sq, sizeof(double),
                              cudaMemcpyHostToDevice, ctx->stream));
   else if (!fused_unfold)
     TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, &a.b.state->xnorm_sq));
-  for (int m = 0; m < ndim; ++m)
-    TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
-                        a.b.grams + (size_t)m * R * R, false));
+  if (!fused_unfold)
+    for (int m = 0; m < ndim; ++m)
+      TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
+                          a.b.grams + (size_t)m * R * R, false));
 
   const bool time_limited = time_limit_s >= 0.0;
   bool stopped_by_time = false;
