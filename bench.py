@@ -463,7 +463,7 @@ def run_ours(args):
     # DRAM bytes (read + write) of one launch of this kernel, mode 0, from the
     # ncu capture summarised in profiles/mttkrp_bf16x3_256_r64_mode0.md (the
     # three modes move the same bytes at this shape)
-    traffic = 67_302_912 + 1_162_240
+    traffic = 67_304_192 + 788_480
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes",
                 "algorithmic_bytes": alg_bytes,
