@@ -740,19 +740,39 @@ mttkrp_bf16x3_runs_kernel(const __grid_constant__ CUtensorMap map_hi,
     // The warp's 32 rows are contiguous in the partials (row stride R): stage
     // them through the A ring (every copy into it was consumed by an MMA
     // that completed before the last acc_full) and store whole rows,
-    // coalesced. Row stride 65 floats keeps both shared accesses conflict-free.
+    // coalesced. With R % 4 == 0 the rows are staged at a 68-float stride
+    // (16-byte aligned; 128-bit shared accesses conflict-free per quarter-warp)
+    // and stored as float4, a warp covering 512 contiguous bytes per store;
+    // else at a 65-float stride, one float per lane.
     const int64_t row0 = m0 + q * 32;
     if (ok) {
-      float* stg = reinterpret_cast<float*>(a_base) + q * (32 * 65);
+      float* stg = reinterpret_cast<float*>(a_base) + q * (32 * 68);
       fence_proxy_async_smem();
-#pragma unroll
-      for (int n = 0; n < 64; ++n)
-        if (n < R) stg[lane * 65 + n] = acc[n];
-      __syncwarp();
       float* out0 = p.partials + (int64_t)blockIdx.x * p.rows * R + row0 * R;
       const int nrows = (int)(p.rows - row0 < 32 ? p.rows - row0 : 32);
-      for (int i = 0; i < nrows; ++i)
-        for (int c = lane; c < R; c += 32) out0[(int64_t)i * R + c] = stg[i * 65 + c];
+      if ((R & 3) == 0) {
+#pragma unroll
+        for (int n = 0; n < 64; n += 4)
+          if (n < R)
+            *reinterpret_cast<float4*>(stg + lane * 68 + n) =
+                make_float4(acc[n], acc[n + 1], acc[n + 2], acc[n + 3]);
+        __syncwarp();
+        const int r4 = R >> 2;  // float4 per row
+        const int total = nrows * r4;
+        float4* o4 = reinterpret_cast<float4*>(out0);
+#pragma unroll 4
+        for (int f = lane; f < total; f += 32) {
+          const int i = f / r4, c4 = f - i * r4;
+          o4[f] = *reinterpret_cast<const float4*>(stg + i * 68 + 4 * c4);
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < 64; ++n)
+          if (n < R) stg[lane * 65 + n] = acc[n];
+        __syncwarp();
+        for (int i = 0; i < nrows; ++i)
+          for (int c = lane; c < R; c += 32) out0[(int64_t)i * R + c] = stg[i * 65 + c];
+      }
     } else {
       if (lane == 0) atomicOr(p.status, DS_TIMEOUT);
       if (row < p.rows) {
