@@ -35,6 +35,20 @@ SEED = 0xC2
 WORKLOAD = "dense CP-ALS 256x256x256 rank 64, 10 iterations, tol 0"
 
 
+def measured_peaks() -> dict:
+    """The pool's measured peaks (HBM copy GB/s, bf16 TFLOP/s), {} if absent."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def hbm_peak_gbs() -> float:
+    """Measured HBM copy bandwidth, else the pool's earlier fallback figure."""
+    return float(measured_peaks().get("hbm_gbs", 6650.0))
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -216,7 +230,7 @@ def run_sparse(tb, torch, ctx, stream, args, world, dist):
             "iter_per_s": iters * world / (ms / 1e3), "ms_per_run": ms, "fit": fit,
             "iters": iters, "synth_s": t1 - t0, "dedup_s": t2 - t1, "csf_build_s": t3 - t2,
             "mttkrp": modes,
-            "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / 6549.4}
+            "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / hbm_peak_gbs()}
 
 
 AD_SHAPE = (128, 96, 64, 48)
@@ -452,13 +466,8 @@ def run_ours(args):
     kernel_ms = sum(kms) / len(kms)
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
     alg_bytes = 4 * n + 3 * SHAPE[0] * RANK * 4  # fp32 tensor + factors (B_min per MTTKRP)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peaks = measured_peaks()
+    peak = hbm_peak_gbs()
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     # DRAM bytes (read + write) of one launch of this kernel, mode 0, from the
     # ncu capture summarised in profiles/mttkrp_bf16x3_256_r64_mode0.md (the

@@ -33,6 +33,15 @@ from .sparse import (  # noqa: F401
     synth_zipf_coo_dev,
 )
 
+from .sparse_io import (  # noqa: F401
+    MatrixMarketHeader,
+    SparseIoError,
+    read_matrix_market,
+    read_tns,
+    write_matrix_market,
+    write_tns,
+)
+
 from .adjoint import (  # noqa: F401
     CpReconstructionGrad,
     CpReconstructionOp,

@@ -29,13 +29,21 @@ def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + [
+def _shared_deps():
+    """Files every translation unit depends on (headers and the flags here)."""
+    return glob.glob(os.path.join(CSRC, "*.cuh")) + [
         os.path.join(ROOT, "include", "tenrso_b200.h"), __file__]
+
+
+def _newer(path: str, deps) -> bool:
+    if not os.path.exists(path):
+        return True
+    t = os.path.getmtime(path)
     return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _stale() -> bool:
+    return _newer(LIB, sources() + _shared_deps())
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -45,14 +53,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
+    shared = _shared_deps()
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        # an object is rebuilt when its source, a shared header or these
+        # flags changed since it was compiled
+        if not (force or verbose) and not _newer(obj, [src] + shared):
+            continue
         cmd = [NVCC, *FLAGS, "-c", src, "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                             stderr=subprocess.STDOUT)))
-        objs.append(obj)
     failed = False
     for src, p in procs:
         out, _ = p.communicate()
