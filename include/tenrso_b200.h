@@ -44,7 +44,9 @@ typedef enum tsr_status {
   TSR_E_UNSUPPORTED = 14,    /* shape/rank outside what the kernels implement */
   TSR_E_COLS_MISMATCH = 15,  /* khatri_rao.rs:63-67 "Number of columns must match" */
   TSR_E_SHAPE = 16,          /* cp/types.rs:24 CpError::ShapeMismatch / coo.rs errors */
-  TSR_E_INDEX_OOB = 17       /* coo.rs:130-137 CooError::IndexOutOfBounds */
+  TSR_E_INDEX_OOB = 17,      /* coo.rs:130-137 CooError::IndexOutOfBounds */
+  TSR_E_NONNEG_VIOLATION = 18, /* cp/types.rs:30-31 CpError::NonnegativeViolation */
+  TSR_E_INVALID_REGULARIZATION = 19 /* cp/types.rs:33-34 CpError::InvalidRegularization */
 } tsr_status;
 
 /* Arithmetic of the dense MTTKRP. FP32: IEEE fp32 FMA on the SIMT pipes.
@@ -162,6 +164,42 @@ int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
                        int64_t rank, int max_iters, double tol, const float* d_init,
                        int precision, double time_limit_s, float* d_out_factors,
                        tsr_cp_info* info);
+
+/* Constraints of cp_als_constrained (crates/tenrso-decomp/src/cp/types.rs:199-225,
+ * core.rs:225-400) in the form the sweep applies them:
+ *   l2  effective_l2() (types.rs:298-303): added to the diagonal of the Gram
+ *       Hadamard before the solve (core.rs:336-343);
+ *   l1  effective_l1() (types.rs:306-308): soft threshold of each new factor
+ *       entry after the solve (core.rs:350-353, helpers.rs:610-623);
+ *   nonnegative: initial factors and every new factor clamped at zero
+ *       (core.rs:271-276, 356-359);
+ *   validate_nonneg_input: with nonnegative, a tensor holding a negative
+ *       entry is rejected with TSR_E_NONNEG_VIOLATION (core.rs:265-267,
+ *       helpers.rs:705-716).
+ * l2 or l1 negative or not finite gives TSR_E_INVALID_REGULARIZATION.
+ * Orthogonality (QR after each update) and Tikhonov of order > 0 are not
+ * applied by the GPU sweep; the host layer rejects them. */
+typedef struct tsr_cp_constraints {
+  double l2;
+  double l1;
+  int nonnegative;
+  int validate_nonneg_input;
+} tsr_cp_constraints;
+
+/* cp_als_constrained (core.rs:225-400) on the dense path; arguments as
+ * tsr_cp_als_f32, plus the constraints (NULL = none, i.e. cp_als). */
+int tsr_cp_als_constrained_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                               int64_t rank, int max_iters, double tol,
+                               const float* init_factors, uint64_t seed,
+                               const tsr_cp_constraints* constraints, int precision,
+                               double time_limit_s, float* out_factors, tsr_cp_info* info);
+/* Device-resident form; arguments as tsr_cp_als_dev_f32 plus the constraints. */
+int tsr_cp_als_constrained_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
+                                   const int64_t* shape, int64_t rank, int max_iters,
+                                   double tol, const float* d_init,
+                                   const tsr_cp_constraints* constraints, int precision,
+                                   double time_limit_s, float* d_out_factors,
+                                   tsr_cp_info* info);
 
 /* ---- sparse: crates/tenrso-sparse --------------------------------------
  * COO entries are `indices` (nnz x ndim, row-major int64) and `values`

@@ -158,6 +158,63 @@ def cp_als(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
     return out, info
 
 
+def cp_als_constrained(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
+                       l2: float = 0.0, l1: float = 0.0, nonneg: bool = False):
+    """Restated ``cp_als_constrained`` (cp/core.rs:225-400) in FP64 from
+    injected factors, for small tensors: per mode MTTKRP (the restated C
+    kernel), Hadamard of the other Grams, ridge l2 on its diagonal
+    (core.rs:336-343), the restated solve, soft threshold by l1
+    (helpers.rs:610-623), projection onto >= 0 (core.rs:356-359); the fit and
+    stopping rules of core.rs:366-392 (the same as cp_als). The input
+    non-negativity check and the initial projection (core.rs:265-276) are
+    applied too. Returns (factors, info dict)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    if nonneg and (X < 0).any():
+        raise ValueError("Non-negative constraint violated: input tensor contains negative values")
+    U = [np.array(f, dtype=np.float64) for f in init_factors]
+    if nonneg:
+        U = [np.maximum(f, 0.0) for f in U]
+    xn = float(np.sum(X * X))
+    prev_fit, fit, osc, change, reason = 0.0, 0.0, 0, 0.0, "MaxIterations"
+    hist, iters = [], 0
+    for it in range(max_iters):
+        iters = it + 1
+        for n in range(X.ndim):
+            M = mttkrp(X, U, n)
+            G = np.ones((rank, rank))
+            for m in range(X.ndim):
+                if m != n:
+                    G *= gram(U[m])
+            if l2 > 0.0:
+                G[np.diag_indices(rank)] += l2
+            U[n] = solve(M, G)
+            if l1 > 0.0:
+                U[n] = np.where(U[n] > l1, U[n] - l1, np.where(U[n] < -l1, U[n] + l1, 0.0))
+            if nonneg:
+                U[n] = np.maximum(U[n], 0.0)
+        # compute_fit (helpers.rs:513-579)
+        inner = float(np.sum(mttkrp(X, U, 0) * U[0]))
+        H = np.ones((rank, rank))
+        for f in U:
+            H *= gram(f)
+        err = np.sqrt(max(xn + float(H.sum()) - 2.0 * inner, 0.0))
+        fit = min(max(1.0 - err / np.sqrt(xn), 0.0), 1.0)
+        hist.append(fit)
+        if it > 0 and fit < prev_fit:
+            osc += 1
+        change = abs(fit - prev_fit)
+        if it > 0 and change < tol:
+            reason = "FitTolerance"
+            break
+        if osc > 5 and it > 10:
+            reason = "Oscillation"
+            break
+        prev_fit = fit
+    info = dict(fit=fit, iters=iters, reason=reason, oscillation_count=osc, oscillated=osc > 0,
+                final_fit_change=change, fit_history=np.asarray(hist))
+    return U, info
+
+
 def coo_deduplicate(idx: np.ndarray, vals: np.ndarray):
     """Restated ``CooTensor::deduplicate`` (coo.rs:320-347)."""
     idx = np.ascontiguousarray(idx, dtype=np.int64).copy()

@@ -33,6 +33,13 @@ from .sparse import (  # noqa: F401
     synth_zipf_coo_dev,
 )
 
+from .constrained import (  # noqa: F401
+    CpConstraints,
+    RegularizationType,
+    cp_als_constrained,
+    cp_als_constrained_dev,
+)
+
 from .sparse_io import (  # noqa: F401
     MatrixMarketHeader,
     SparseIoError,

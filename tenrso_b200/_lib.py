@@ -17,6 +17,16 @@ I64 = C.c_int64
 PI64 = C.POINTER(C.c_int64)
 
 
+class CpConstraintsC(C.Structure):
+    """tsr_cp_constraints: the reduced form of CpConstraints the sweep applies."""
+    _fields_ = [
+        ("l2", C.c_double),
+        ("l1", C.c_double),
+        ("nonnegative", C.c_int),
+        ("validate_nonneg_input", C.c_int),
+    ]
+
+
 class CpInfo(C.Structure):
     _fields_ = [
         ("fit", C.c_double),
@@ -53,6 +63,12 @@ SIGNATURES = {
                                  C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
     "tsr_cp_als_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_int,
                                      C.c_double, P, C.POINTER(CpInfo)]),
+    "tsr_cp_als_constrained_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
+                                             C.c_uint64, C.POINTER(CpConstraintsC), C.c_int,
+                                             C.c_double, P, C.POINTER(CpInfo)]),
+    "tsr_cp_als_constrained_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
+                                                 C.POINTER(CpConstraintsC), C.c_int, C.c_double,
+                                                 P, C.POINTER(CpInfo)]),
     "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_coo_deduplicate_f32": (C.c_int, [P, P, P, I64, C.c_int, P, PI64]),
     "tsr_csf_from_coo_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, P, P, P, P]),
@@ -118,7 +134,7 @@ STATUS = {
     7: "TSR_E_NOT_SPD", 8: "TSR_E_TIMEOUT", 9: "TSR_E_CUDA", 10: "TSR_E_INVALID_ARG",
     11: "TSR_E_NEED_2_FACTORS", 12: "TSR_E_TILE_SIZE", 13: "TSR_E_MODE_ORDER",
     14: "TSR_E_UNSUPPORTED", 15: "TSR_E_COLS_MISMATCH", 16: "TSR_E_SHAPE",
-    17: "TSR_E_INDEX_OOB",
+    17: "TSR_E_INDEX_OOB", 18: "TSR_E_NONNEG_VIOLATION", 19: "TSR_E_INVALID_REGULARIZATION",
 }
 
 

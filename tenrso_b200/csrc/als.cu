@@ -310,6 +310,20 @@ __device__ void fit_update(const AlsBuffers& b, double tol) {
   __syncthreads();
 }
 
+__global__ void clamp_nonneg_kernel(float* __restrict__ U, int64_t n) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    U[e] = fmaxf(U[e], 0.f);
+}
+
+__global__ void any_negative_kernel(const float* __restrict__ X, int64_t n, int* flag) {
+  bool neg = false;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    neg |= __ldg(X + e) < 0.f;
+  if (__any_sync(0xffffffffu, neg) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
 __global__ void fit_kernel(AlsBuffers b, double tol) {
   AlsState* st = b.state;
   if (st->done || !st->fit_pending) return;
@@ -321,7 +335,8 @@ __global__ void fit_kernel(AlsBuffers b, double tol) {
 // accumulator (and <X,Xhat> for the last mode) for the solve that follows.
 template <int RB>
 __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
-                                                   float ridge_eps, int last, double tol) {
+                                                   float ridge_eps, int last, double tol,
+                                                   double l2) {
   __shared__ GjShared<RB> gsh;
   AlsState* st = b.state;
   if (st->done) return;
@@ -333,13 +348,13 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
   }
   const int RR = R * R;
   double a[RB][RB];
-  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
+  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, l2, a, true);
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
   bool ok = gj_inverse<RB>(a, gsh);
   if (!ok) {
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, l2 + (double)ridge_eps, a, false);
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
   }
@@ -358,8 +373,8 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
       if (threadIdx.x == 0) gsh.scale = d / R;
     }
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps * fmax(gsh.scale, 1.0),
-                      a, false);
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R,
+                      l2 + (double)ridge_eps * fmax(gsh.scale, 1.0), a, false);
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 2;
   }
@@ -416,7 +431,7 @@ template <int RB>
 __global__ void __launch_bounds__(256)
 solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
              int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
-             double tol) {
+             double tol, float l1, int nonneg) {
   extern __shared__ __align__(16) double sh[];
   __shared__ __align__(8) uint64_t gi_bar;
   __shared__ int gi_state;  // 0 copy in flight, 1 landed, 2 gave up
@@ -555,7 +570,11 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
         s3 += Ms[i * R + k + 3] * Gi[(k + 3) * R + c];
       }
       for (; k < R; ++k) s0 += Ms[i * R + k] * Gi[k * R + c];
-      const float v = (float)((s0 + s1) + (s2 + s3));
+      float v = (float)((s0 + s1) + (s2 + s3));
+      // cp_als_constrained: soft threshold (helpers.rs:610-623), then the
+      // projection onto v >= 0 (core.rs:356-359)
+      if (l1 > 0.f) v = v > l1 ? v - l1 : (v < -l1 ? v + l1 : 0.f);
+      if (nonneg) v = fmaxf(v, 0.f);
       U[(r0 + i) * R + c] = v;
       Us[e] = (double)v;
       ip += Ms[e] * (double)v;
@@ -667,18 +686,36 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 }
 
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last, double tol) {
+                float ridge_eps, bool last, double tol, double l2) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const int lst = last ? 1 : 0;
   switch ((R + 15) / 16) {
-    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
-    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol); break;
+    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
   }
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_clamp_nonneg(tsr_ctx* ctx, cudaStream_t s, float* U, int64_t n) {
+  if (n <= 0) return TSR_OK;
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(n, 256), 4 * (int64_t)ctx->sm_count);
+  clamp_nonneg_kernel<<<grid, 256, 0, s>>>(U, n);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+int launch_any_negative(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, int* flag) {
+  if (n <= 0) return TSR_OK;
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(n, 256), 4 * (int64_t)ctx->sm_count);
+  any_negative_kernel<<<grid, 256, 0, s>>>(X, n, flag);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
@@ -693,7 +730,7 @@ int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int 
 
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
-                 double tol) {
+                 double tol, float l1, int nonneg) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   // about 64 row chunks (one per CTA) for small modes, so that the Gram
   // atomics stay few; 16-row chunks grid-strided over at most 8 CTAs per SM
@@ -708,7 +745,7 @@ int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float*
   const int lst = last ? 1 : 0;
 #define TSR_SOLVE(RB)                                                                    \
   TSR_CUDA(launch_pdl(solve_kernel<RB>, dim3(grid), dim3(256), smem, s, b, partials, splits, \
-                      rows, R, rpc, U, gram, lst, ndim, tol))
+                      rows, R, rpc, U, gram, lst, ndim, tol, l1, nonneg))
   switch ((R + 15) / 16) {
     case 1: TSR_SOLVE(1); break;
     case 2: TSR_SOLVE(2); break;

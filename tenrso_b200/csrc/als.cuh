@@ -71,15 +71,24 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 // Hadamard of all Grams except `mode`, its inverse (ridge retry), and the
 // zeroing of gram[mode] (and, when `last`, state->inner) before the solve.
 // For mode 0 it first forms the fit of the previous sweep, when one is pending.
+// l2 >= 0 is added to the Hadamard's diagonal before the inverse (the ridge of
+// cp_als_constrained, core.rs:336-343); the stored Hadamard (used by the fit)
+// stays unshifted.
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last, double tol);
+                float ridge_eps, bool last, double tol, double l2 = 0.0);
+// Clamp n floats at zero (non-negative initial factors, core.rs:271-276).
+int launch_clamp_nonneg(tsr_ctx* ctx, cudaStream_t s, float* U, int64_t n);
+// Sets *flag to 1 if any of the n values is negative (helpers.rs:705-716).
+int launch_any_negative(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, int* flag);
 // The pending fit of the last sweep (fit, history, stopping rules).
 int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int R, double tol);
 // U_mode = (sum of split partials) . G^{-1} and its Gram U^T U added into
 // `gram` (zeroed by this mode's launch_chol); `last` also accumulates <M, U>
-// and marks the sweep's fit pending.
+// and marks the sweep's fit pending. Each new fp32 entry is soft-thresholded
+// by l1 when l1 > 0 and clamped at zero when nonneg (core.rs:350-359) before
+// it is stored and enters the Gram and the fit.
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
-                 double tol);
+                 double tol, float l1 = 0.f, int nonneg = 0);
 
 }  // namespace tsr

@@ -223,6 +223,9 @@ struct SweepArgs {
   int precision;
   double tol;
   float ridge;
+  double l2;   // cp_als_constrained: Gram ridge, soft threshold, projection
+  float l1;
+  int nonneg;
   FactorTable ft;
   const void* op_ptrs[3 * kMaxModes];
   float* partials;
@@ -237,7 +240,7 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
   TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[0], 0));
   for (int n = 0; n < a.ndim; ++n) {
     const bool last = n == a.ndim - 1;
-    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last, a.tol));
+    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last, a.tol, a.l2));
     TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
     float* partials = a.partials;
     int splits = 1;
@@ -248,7 +251,7 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
     TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
     TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
                          const_cast<float*>(a.ft.ptr[n]), a.b.grams + (size_t)n * a.R * a.R,
-                         last, a.ndim, a.tol));
+                         last, a.ndim, a.tol, a.l1, a.nonneg));
     if (!last) {  // the next inverse needs this mode's Gram
       TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
       TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
@@ -260,7 +263,7 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
 int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
                   const int64_t* shape, int64_t rank, int max_iters, double tol,
                   const float* d_init, int precision, double time_limit_s, float* d_out,
-                  tsr_cp_info* info) {
+                  tsr_cp_info* info, const tsr_cp_constraints* cons = nullptr) {
   auto t_start = std::chrono::steady_clock::now();
   // core.rs:82-94
   if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
@@ -275,6 +278,15 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
                 kMaxRank);
   if (ndim < 2 && max_iters > 0)
     return fail(TSR_E_SHAPE, "Shape mismatch: Need at least 2 factor matrices for MTTKRP");
+  if (cons) {  // types.rs:105-182 (validate), core.rs:262-267
+    if (sp) return fail(TSR_E_UNSUPPORTED, "constraints apply to the dense CP-ALS only");
+    if (!(cons->l2 >= 0.0) || !std::isfinite(cons->l2))
+      return fail(TSR_E_INVALID_REGULARIZATION,
+                  "Invalid regularization parameter: L2 lambda must be >= 0, got %g", cons->l2);
+    if (!(cons->l1 >= 0.0) || !std::isfinite(cons->l1))
+      return fail(TSR_E_INVALID_REGULARIZATION,
+                  "Invalid regularization parameter: L1 lambda must be >= 0, got %g", cons->l1);
+  }
   const int R = (int)rank;
   const int64_t n = numel(ndim, shape);
 
@@ -288,6 +300,11 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   a.tol = tol;
   a.ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
   a.sp = sp;
+  if (cons) {
+    a.l2 = cons->l2;
+    a.l1 = (float)cons->l1;  // the threshold in the factors' type (core.rs:351)
+    a.nonneg = cons->nonnegative ? 1 : 0;
+  }
 
   // factors live in d_out for the whole run (updated in place)
   int64_t ftotal = 0;
@@ -314,6 +331,18 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   a.b.history = (double*)((char*)stp + 256);
   TSR_CUDA(cudaMemsetAsync(stp, 0, sbytes, ctx->stream));
   TSR_CUDA(cudaMemsetAsync(gp, 0, gbytes, ctx->stream));
+  if (cons && cons->nonnegative && cons->validate_nonneg_input) {
+    // helpers.rs:705-716: one pass over X before any factor is touched
+    TSR_TRY(launch_any_negative(ctx, ctx->stream, dX, n, &a.b.state->pad));
+    int neg = 0;
+    TSR_CUDA(cudaMemcpyAsync(&neg, &a.b.state->pad, sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (neg)
+      return fail(TSR_E_NONNEG_VIOLATION,
+                  "Non-negative constraint violated: input tensor contains negative values");
+  }
+  if (a.nonneg) TSR_TRY(launch_clamp_nonneg(ctx, ctx->stream, d_out, ftotal));
 
   // per-mode unfoldings, resident for the whole run (the reference re-unfolds
   // in every mttkrp call, mttkrp.rs:126)
@@ -657,6 +686,28 @@ int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* s
                    int64_t rank, int max_iters, double tol, const float* init_factors,
                    uint64_t seed, int precision, double time_limit_s, float* out_factors,
                    tsr_cp_info* info) {
+  return tsr_cp_als_constrained_f32(ctx, tensor, ndim, shape, rank, max_iters, tol, init_factors,
+                                    seed, nullptr, precision, time_limit_s, out_factors, info);
+}
+
+int tsr_cp_als_constrained_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
+                                   const int64_t* shape, int64_t rank, int max_iters,
+                                   double tol, const float* d_init,
+                                   const tsr_cp_constraints* constraints, int precision,
+                                   double time_limit_s, float* d_out_factors,
+                                   tsr_cp_info* info) {
+  if (!shape || !d_tensor || !d_init || !d_out_factors)
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  TSR_TRY(check_ctx(ctx));
+  return cp_als_device(ctx, d_tensor, nullptr, ndim, shape, rank, max_iters, tol, d_init,
+                       precision, time_limit_s, d_out_factors, info, constraints);
+}
+
+int tsr_cp_als_constrained_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                               int64_t rank, int max_iters, double tol,
+                               const float* init_factors, uint64_t seed,
+                               const tsr_cp_constraints* constraints, int precision,
+                               double time_limit_s, float* out_factors, tsr_cp_info* info) {
   if (!shape || !tensor || !out_factors) return fail(TSR_E_INVALID_ARG, "null argument");
   if (rank == 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
   for (int d = 0; d < ndim; ++d)
@@ -683,7 +734,7 @@ int tsr_cp_als_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* s
   TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * ftotal, &df));
   TSR_CUDA(cudaMemcpyAsync(df, init, sizeof(float) * ftotal, cudaMemcpyHostToDevice, ctx->stream));
   TSR_TRY(cp_als_device(ctx, dX, nullptr, ndim, shape, rank, max_iters, tol, (const float*)df,
-                        precision, time_limit_s, (float*)df, info));
+                        precision, time_limit_s, (float*)df, info, constraints));
   TSR_CUDA(cudaMemcpyAsync(out_factors, df, sizeof(float) * ftotal, cudaMemcpyDeviceToHost,
                            ctx->stream));
   TSR_CUDA(cudaStreamSynchronize(ctx->stream));
