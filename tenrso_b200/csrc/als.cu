@@ -271,6 +271,17 @@ __device__ void load_hadamard(const double* __restrict__ grams, double* __restri
     }
 }
 
+// a += l2 * I on this thread's RB x RB block (the ridge of cp_als_constrained)
+template <int RB>
+__device__ __forceinline__ void add_diagonal(double (&a)[RB][RB], int R, double l2) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj)
+      if (ty + 16 * ai == tx + 16 * bj && ty + 16 * ai < R) a[ai][bj] += l2;
+}
+
 // fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
 // core.rs:142-166) of the sweep whose last solve has finished, from the
 // scalars that solve accumulated: ||X||^2 + ||Xhat||^2 - 2 <X, Xhat>. Called
@@ -348,13 +359,15 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
   }
   const int RR = R * R;
   double a[RB][RB];
-  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, l2, a, true);
+  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
+  if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
   bool ok = gj_inverse<RB>(a, gsh);
   if (!ok) {
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, l2 + (double)ridge_eps, a, false);
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
+    if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
   }
@@ -373,8 +386,9 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
       if (threadIdx.x == 0) gsh.scale = d / R;
     }
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R,
-                      l2 + (double)ridge_eps * fmax(gsh.scale, 1.0), a, false);
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps * fmax(gsh.scale, 1.0),
+                      a, false);
+    if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 2;
   }
