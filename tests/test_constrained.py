@@ -82,12 +82,15 @@ def test_constrained_fit_vs_oracle(orc, precision, name, c, kw):
 
 @pytest.mark.gpu
 def test_no_constraints_equals_cp_als():
+    """Same kernels and sweep graph; the Grams and the fit are FP64 atomic
+    sums across CTAs, so two runs agree to FP64 rounding, not bit for bit."""
     X, init = _case((32, 24, 20), 4, 7, "normal")
     a = tb.cp_als(X, 4, 8, 0.0, init=init)
     b = tb.cp_als_constrained(X, 4, 8, 0.0, init=init, constraints=CC())
-    assert a.fit == b.fit
+    assert a.iters == b.iters == 8
+    assert abs(a.fit - b.fit) <= 1e-12
     for x, y in zip(a.factors, b.factors):
-        assert np.array_equal(x, y)
+        assert np.allclose(x, y, rtol=1e-5, atol=1e-6)
 
 
 @pytest.mark.gpu
