@@ -44,6 +44,17 @@ def measured_peaks() -> dict:
         return {}
 
 
+def max_over_ranks(x: float, dist, device="cuda") -> float:
+    """The largest value of x over all ranks (identity without a process group).
+    Every rank must call it at the same point: it is a collective."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def hbm_peak_gbs() -> float:
     """Measured HBM copy bandwidth, else the pool's earlier fallback figure."""
     return float(measured_peaks().get("hbm_gbs", 6650.0))
@@ -208,10 +219,7 @@ def run_sparse(tb, torch, ctx, stream, args, world, dist):
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / steps
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     d_factors = [dinit.data_ptr() + 4 * sum(SP_SHAPE[:m]) * SP_RANK for m in range(3)]
     modes = []
     for mode in range(3):
@@ -271,10 +279,7 @@ def run_adjoint(tb, torch, ctx, stream, args, world, dist, rank):
         ev1.record(stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1) / steps
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         return ms, (ctx.launches - l0) // steps
 
     for prec in ("fp32", "bf16x3"):
@@ -349,10 +354,7 @@ def run_batched(tb, torch, ctx, stream, args, world, dist, rank):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / steps
     launches = (ctx.launches - l0) // steps
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     info = b.cp_als_dev(BT_ITERS, 0.0, d_init.data_ptr(), d_out.data_ptr(), want_info=True)
     elems = [X.size for X in tensors]
     # two passes over each tensor per sweep, 4 bytes per element
@@ -429,10 +431,7 @@ def run_ours(args):
         ev1.record(stream)
         barrier()
         ms = ev0.elapsed_time(ev1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         return ms, res, ctx.launches - l0
 
     for _ in range(args.warmup):
@@ -490,11 +489,7 @@ def run_ours(args):
         tb.cp_als(Xp, RANK, ITERS, 0.0, init=initp, precision="bf16x3", ctx=ctx)
     barrier()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_wall = [e2e_s]
-    if dist is not None:
-        t = torch.tensor(e2e_wall, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     e2e = {"value": ITERS * world / e2e_s, "unit": "iter/s",
            "h2d_bytes_per_step": int(X.nbytes + flat_init.nbytes),
            "d2h_bytes_per_step": int(flat_init.nbytes + 64),
