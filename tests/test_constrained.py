@@ -124,3 +124,22 @@ def test_constrained_dev_and_negative_init(orc):
                                      nonneg=True)
     assert iters == 6 and abs(fit - info["fit"]) <= 1e-4
     assert (do.cpu().numpy() >= 0).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rank,precision", [(40, "fp32"), (64, "bf16x3")])
+def test_constrained_large_rank_vs_oracle(orc, rank, precision):
+    """Ranks above 16 run the multi-block (RB = 3, 4) inverse and solve
+    instances, whose diagonal blocks take the ridge."""
+    X, init = _case((96, 80, 72), rank, 0xC2 + rank, "uniform")
+    c = CC(nonnegative=True, l2_reg=0.5)
+    res = tb.cp_als_constrained(X, rank, 6, 0.0, init=init, constraints=c, precision=precision)
+    U, info = orc.cp_als_constrained(X, rank, 6, 0.0, [f.astype(np.float64) for f in init],
+                                     l2=0.5, nonneg=True)
+    assert res.iters == info["iters"] == 6
+    assert abs(res.fit - info["fit"]) <= 1e-4, (rank, precision, res.fit, info["fit"])
+    assert all((f >= 0).all() for f in res.factors)
+    # factors of U(0,1) data at rank 40-64 are less well conditioned than
+    # the fit; fp32 rounding in six sweeps moves them by up to about 1e-2
+    for a, b in zip(res.factors, U):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 2e-2
