@@ -176,13 +176,58 @@ def _write_lines(dst, lines) -> None:
         dst.write(text)
 
 
+def _tns_columns(src):
+    """Fast path: pandas' C tokenizer over whitespace-separated columns, or
+    None when the text is anything but well-formed integer indices and a
+    numeric value (the line-by-line reader then gives the exact error)."""
+    try:
+        import pandas as pd
+    except ImportError:
+        return None
+    try:
+        df = pd.read_csv(src, sep=r"\s+", header=None, comment="#", engine="c",
+                         skip_blank_lines=True)
+    except Exception:
+        return None
+    if df.shape[1] < 2 or df.isna().to_numpy().any():
+        return None
+    from pandas.api.types import is_integer_dtype, is_numeric_dtype
+    idx = df.iloc[:, :-1]
+    if not all(is_integer_dtype(t) for t in idx.dtypes):
+        return None
+    if not is_numeric_dtype(df.dtypes.iloc[-1]):
+        return None
+    idx = idx.to_numpy(np.int64)
+    if idx.size and idx.min() < 1:
+        return None
+    return idx - 1, df.iloc[:, -1].to_numpy(np.float64)
+
+
 def read_tns(src, shape: Optional[Sequence[int]] = None) -> CooTensor:
     """Read a FROSTT `.tns` tensor: one entry per line, N 1-based indices then
     the value; blank lines and lines starting with `#` or `%` are skipped.
 
     The order N is taken from the first entry and must be the same on every
     line. `shape` defaults to the largest index seen in each mode. Entries
-    stay in file order (duplicates are kept for `CooTensor.deduplicate`)."""
+    stay in file order (duplicates are kept for `CooTensor.deduplicate`).
+    Large files are tokenised by pandas' C parser when it is installed; any
+    irregular text goes through the line-by-line reader below."""
+    if isinstance(src, (bytes, bytearray)):
+        src = io.StringIO(bytes(src).decode())
+    elif not isinstance(src, (str, os.PathLike)):
+        src = io.StringIO(_open_text(src).read())  # replayable for the fallback
+    cols = _tns_columns(src)
+    if cols is not None:
+        idx, vals = cols
+        ndim = idx.shape[1]
+        if shape is None:
+            shape = (idx.max(axis=0) + 1).tolist() if len(idx) else None
+        if shape is not None and len(shape) != ndim:
+            raise _conversion(f"Shape has {len(shape)} modes but the entries have {ndim} indices")
+        if shape is not None:
+            return CooTensor(idx, vals.astype(np.float32), list(shape))
+    if isinstance(src, io.StringIO):
+        src.seek(0)
     f = _open_text(src)
     close = isinstance(src, (str, os.PathLike))
     ndim = None

@@ -144,3 +144,28 @@ def test_tns_shape_inference_comments_and_errors():
     with pytest.raises(tb.SparseIoError, match="Shape has 2 modes"):
         tb.read_tns(io.StringIO("1 1 1 2.0\n"), shape=(2, 2))
     assert tb.read_tns(io.StringIO(""), shape=(2, 3)).nnz() == 0
+
+
+def test_tns_fast_and_line_readers_agree(tmp_path, monkeypatch):
+    rng = np.random.default_rng(9)
+    shape = (50, 40, 30, 20)
+    idx = np.stack([rng.integers(0, n, 20000) for n in shape], axis=1)
+    vals = (rng.standard_normal(20000) * 10).astype(np.float32)
+    path = tmp_path / "x.tns"
+    tb.write_tns(tb.CooTensor(idx, vals, shape), str(path))
+    fast = tb.read_tns(str(path))
+    from tenrso_b200 import sparse_io
+    monkeypatch.setattr(sparse_io, "_tns_columns", lambda src: None)
+    slow = tb.read_tns(str(path))
+    assert fast.shape() == slow.shape() == [int(i) + 1 for i in idx.max(axis=0)]
+    assert np.array_equal(fast.indices(), slow.indices())
+    assert np.array_equal(fast.values(), slow.values())
+    assert np.array_equal(fast.values(), vals)
+
+
+def test_tns_irregular_text_takes_the_line_reader():
+    # '%' comments and integer-looking values parse the same either way
+    coo = tb.read_tns(io.StringIO("% header\n1 2 3\n2 1 4\n"))
+    assert coo.shape() == [2, 2] and coo.values().tolist() == [3.0, 4.0]
+    with pytest.raises(tb.SparseIoError, match="Invalid value"):
+        tb.read_tns(b"1 1 x\n")
