@@ -131,19 +131,21 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
                                double* ms_per_launch, int64_t* splits_out);
 
 /* Allocation-free MTTKRP of mode 0 (FP32 split-K path). No tenrso
- * counterpart: it exists for callers that cannot call cudaMalloc (code whose
- * device memory is owned by another framework's caching allocator, or code
- * that enqueues work during CUDA-graph stream capture). It takes a stream
- * instead of a tsr_ctx and keeps its split partials in a fixed 16 MiB
+ * counterpart: it exists for callers that cannot call cudaMalloc, such as a
+ * library whose host application's caching allocator owns all device memory,
+ * or a service that sizes every device buffer before it starts. It takes a
+ * stream instead of a tsr_ctx and keeps its split partials in a fixed 16 MiB
  * device array that every GPU loading the library holds until exit; it calls
  * no cudaMalloc/cudaFree. Device pointers, row-major layouts as
  * tsr_mttkrp_dev_f32; needs prod(shape[1:]) % 4 == 0 and a 16-byte aligned
  * tensor, and rejects with TSR_E_UNSUPPORTED any problem whose split partials
  * (shape[0] x rank x the kernel's split count) exceed the array's 4 Mi
- * floats. The first call on a device
- * resolves the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture. All calls share the array, so calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * floats. The stream must belong to the current device (TSR_E_INVALID_ARG
+ * otherwise); negative sizes are rejected, and an empty tensor gives a zero
+ * output. The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race and must
+ * be serialised by the caller. */
 int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
                                  const int64_t* shape, const float* const* d_factors,
                                  int64_t rank, float* d_out);

@@ -10,6 +10,8 @@ namespace tsr {
 int validate_mttkrp(int ndim, const int64_t* shape, int n_factors, const int64_t* frows,
                     const int64_t* fcols, int mode);
 int check_precision(int precision);
+// Negative mode sizes (TSR_E_INVALID_ARG) or rank (TSR_E_INVALID_RANK).
+int check_sizes(int ndim, const int64_t* shape, int64_t rank);
 int64_t numel(int ndim, const int64_t* shape);
 
 // Host tensor (any strides) into the context's tensor slot as row-major fp32.

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 
 #include "als.cuh"
 #include "csf.cuh"
@@ -38,6 +39,14 @@ int validate_mttkrp(int ndim, const int64_t* shape, int n_factors, const int64_t
   if (ndim < 2) return fail(TSR_E_NEED_2_FACTORS, "Need at least 2 factor matrices for MTTKRP");
   if (ndim > kMaxModes)
     return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", ndim, kMaxModes);
+  return TSR_OK;
+}
+
+int check_sizes(int ndim, const int64_t* shape, int64_t rank) {
+  for (int d = 0; d < ndim; ++d)
+    if (shape[d] < 0)
+      return fail(TSR_E_INVALID_ARG, "mode %d has a negative size (%lld)", d, (long long)shape[d]);
+  if (rank < 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
   return TSR_OK;
 }
 
@@ -515,16 +524,23 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   return TSR_OK;
 }
 
+// cudaFuncSetAttribute acts on the current device's context, so the raised
+// shared-memory limits are set once per device (guarded: several host threads
+// may make their first call at the same time).
 void init_kernel_attributes() {
-  static bool done = false;
-  if (done) return;
+  static std::mutex mu;
+  static uint64_t done_mask = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done_mask & (1ull << dev)) return;
   init_tc_attributes();
   init_simt_attributes();
   init_als_attributes();
   init_adjoint_attributes();
   init_csf_attributes();
   init_batched_attributes();
-  done = true;
+  done_mask |= 1ull << dev;
 }
 
 }  // namespace tsr
@@ -562,6 +578,7 @@ int tsr_mttkrp_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* s
     return fail(TSR_E_INVALID_ARG, "null argument");
   TSR_TRY(validate_mttkrp(ndim, shape, n_factors, factor_rows, factor_cols, mode));
   TSR_TRY(check_precision(precision));
+  TSR_TRY(check_sizes(ndim, shape, factor_cols[0]));
   TSR_TRY(check_ctx(ctx));
   const int R = (int)factor_cols[0];
   const int64_t nout = shape[mode] * R;
@@ -622,7 +639,14 @@ int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
   std::vector<int64_t> cols(ndim, rank);
   TSR_TRY(validate_mttkrp(ndim, shape, ndim, shape, cols.data(), mode));
   TSR_TRY(check_precision(precision));
+  TSR_TRY(check_sizes(ndim, shape, rank));
   TSR_TRY(check_ctx(ctx));
+  const int64_t nout = shape[mode] * rank;
+  if (nout == 0) return TSR_OK;
+  if (numel(ndim, shape) == 0) {  // an empty sum: the output is zero
+    TSR_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float) * nout, ctx->stream));
+    return TSR_OK;
+  }
   FactorTable ft{};
   for (int m = 0; m < ndim; ++m) {
     ft.ptr[m] = d_factors[m];

@@ -1,13 +1,15 @@
 // An allocation-free dense MTTKRP entry point.
 //
-// Some callers cannot call cudaMalloc: code that runs under a framework whose
-// caching allocator owns all device memory (a raw cudaMalloc there fragments
-// the pool or is forbidden outright), and code that enqueues work while a
-// stream is being captured into a CUDA graph, where allocation calls are not
-// permitted. For them this entry point runs the FP32 split-K MTTKRP of mode 0
-// with its split partials in a fixed, file-scope device array instead of a
-// context workspace: it makes no cudaMalloc / cudaFree call and needs no
-// tsr_ctx (the caller passes a stream, the inputs and the output).
+// Some callers cannot call cudaMalloc. A library embedded in a framework
+// whose caching allocator owns the GPU's memory must not allocate behind that
+// allocator's back (a raw cudaMalloc fragments its pool, fails once the pool
+// has reserved the device, or is forbidden by the host application outright),
+// and a service that sizes every device buffer up front cannot tolerate a
+// call that may allocate on first use. For them this entry point runs the
+// FP32 split-K MTTKRP of mode 0 with its split partials in a fixed,
+// file-scope device array instead of a context workspace: it makes no
+// cudaMalloc / cudaFree call and needs no tsr_ctx (the caller passes a
+// stream, the inputs and the output).
 //
 // The array below is part of the library image: every GPU that loads the
 // library holds its 16 MiB until the process exits. All calls share it and
@@ -64,7 +66,27 @@ int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
   if (ndim > kMaxModes)
     return fail(TSR_E_UNSUPPORTED, "tensor rank %d exceeds the supported %d", ndim, kMaxModes);
   if (rank <= 0) return fail(TSR_E_INVALID_RANK, "Invalid rank: %lld", (long long)rank);
+  for (int d = 0; d < ndim; ++d)
+    if (shape[d] < 0)
+      return fail(TSR_E_INVALID_ARG, "mode %d has a negative size (%lld)", d, (long long)shape[d]);
+  // the kernels run on the caller's stream, the scratch address and the SM
+  // count come from the current device: both must be the same device
+  int dev = 0;
+  TSR_CUDA(cudaGetDevice(&dev));
+  if (stream) {
+    int sdev = -1;
+    TSR_CUDA(cudaStreamGetDevice((cudaStream_t)stream, &sdev));
+    if (sdev != dev)
+      return fail(TSR_E_INVALID_ARG,
+                  "the stream belongs to device %d but device %d is current", sdev, dev);
+  }
+  const int64_t nout = shape[0] * rank;
+  if (nout == 0) return TSR_OK;
   const Unfolding u = make_unfolding(ndim, shape, 0);
+  if (u.cols == 0) {  // an empty sum over the other modes: the output is zero
+    TSR_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float) * nout, (cudaStream_t)stream));
+    return TSR_OK;
+  }
   if (u.cols % 4 != 0 || ((uintptr_t)d_tensor & 15))
     return fail(TSR_E_UNSUPPORTED,
                 "allocation-free MTTKRP needs the product of the non-leading mode sizes to be a "
@@ -74,8 +96,6 @@ int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
   uu.ld = u.cols;
   tsr_ctx shim;  // launch bookkeeping only: stream and SM count, no allocations
   shim.stream = (cudaStream_t)stream;
-  int dev = 0;
-  TSR_CUDA(cudaGetDevice(&dev));
   TSR_CUDA(cudaDeviceGetAttribute(&shim.sm_count, cudaDevAttrMultiProcessorCount, dev));
   shim.reserve_sms = 0;
   const SplitPlan plan = plan_simt(&shim, u.rows, u.cols, (int)rank);
@@ -85,7 +105,7 @@ int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
                 "allocation-free MTTKRP: %zu partial floats exceed the fixed %zu-float scratch "
                 "(shape[0] x rank x splits too large)",
                 need, kNoAllocScratchFloats);
-  init_kernel_attributes();  // host-side launch attributes, once per process
+  init_kernel_attributes();  // host-side launch attributes, once per device
   float* scratch;
   TSR_TRY(scratch_for_current_device(&scratch));
   FactorTable ft{};

@@ -185,8 +185,11 @@ def _tns_columns(src):
     except ImportError:
         return None
     try:
-        df = pd.read_csv(src, sep=r"\s+", header=None, comment="#", engine="c",
-                         skip_blank_lines=True)
+        # no comment handling here: a '#' or '%' anywhere leaves non-numeric
+        # tokens, and the file goes to the line-by-line reader; values parse
+        # with correct rounding, as Python's float() does there
+        df = pd.read_csv(src, sep=r"\s+", header=None, engine="c", skip_blank_lines=True,
+                         float_precision="round_trip")
     except Exception:
         return None
     if df.shape[1] < 2 or df.isna().to_numpy().any():

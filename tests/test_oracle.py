@@ -184,3 +184,24 @@ def test_cp_vjp_vs_central_differences(orc, shape, R):
         fd = orc.fd_grad_entries(X, fs, 1e-3, m, ent)
         an = np.array([g[m][i, r] for i, r in ent])
         assert np.abs(fd - an).max() <= 1e-7 * np.abs(an).max(), m
+
+
+def test_oracle_reproduces_c2_fit_fixture(orc):
+    """tests/golden/c2_fp64_fit.json (the FP64 fit history the GPU tests and
+    bench.py compare with) is what the oracle computes on the 256^3 rank-64
+    workload. The oracle's fp32 instantiation sits far below it (0.9345 vs
+    0.9700): its sequential f32 sum of squares stagnates at this size
+    (helpers.rs:498-510), so the fp32 reference's own fit is not a parity
+    target there."""
+    import json
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_c2_fit
+    with open(os.path.join(here, "golden", "c2_fp64_fit.json")) as f:
+        ref = json.load(f)
+    got = make_c2_fit.compute()
+    assert np.max(np.abs(np.asarray(got["fp64_fit_history"]) -
+                         np.asarray(ref["fp64_fit_history"]))) <= 1e-12
+    assert abs(got["fp32_fit"] - ref["fp32_fit"]) <= 1e-6

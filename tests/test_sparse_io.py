@@ -169,3 +169,23 @@ def test_tns_irregular_text_takes_the_line_reader():
     assert coo.shape() == [2, 2] and coo.values().tolist() == [3.0, 4.0]
     with pytest.raises(tb.SparseIoError, match="Invalid value"):
         tb.read_tns(b"1 1 x\n")
+
+
+def test_tns_trailing_comment_and_exponents_same_with_and_without_pandas(monkeypatch):
+    """A '#' after the numbers of a data line is an error for both readers, and
+    exponent-form values parse to the same fp32 bits either way."""
+    from tenrso_b200 import sparse_io
+    text = ("1 1 1 1.5e-3\n2 3 1 -7.25E+2\n1 2 2 3.4028234e38\n2 1 2 1e-45\n"
+            "1 3 1 0.1\n2 2 2 123456789.123456789\n")
+    bad = "1 1 1 2.0 # trailing note\n2 2 2 1.0\n"
+    fast = tb.read_tns(io.StringIO(text))
+    with pytest.raises(tb.SparseIoError) as e_fast:
+        tb.read_tns(io.StringIO(bad))
+    monkeypatch.setattr(sparse_io, "_tns_columns", lambda src: None)
+    slow = tb.read_tns(io.StringIO(text))
+    with pytest.raises(tb.SparseIoError) as e_slow:
+        tb.read_tns(io.StringIO(bad))
+    assert str(e_fast.value) == str(e_slow.value)
+    assert fast.shape() == slow.shape()
+    assert np.array_equal(fast.indices(), slow.indices())
+    assert np.array_equal(fast.values().view(np.uint32), slow.values().view(np.uint32))
