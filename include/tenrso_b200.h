@@ -89,6 +89,12 @@ int tsr_ctx_destroy(tsr_ctx* ctx);
 int tsr_ctx_synchronize(tsr_ctx* ctx);
 /* Kernels launched through this context since creation (a counter). */
 int64_t tsr_ctx_launch_count(const tsr_ctx* ctx);
+/* Clock-cycle budget of each bounded pipeline wait in the tensor-core MTTKRP
+ * kernels (cycles <= 0 restores the default, about one second). A wait that
+ * runs out makes the kernel drain its copies, free its tensor memory and
+ * return; the call then fails with TSR_E_TIMEOUT and the context stays usable.
+ * No tenrso counterpart (failure-path testing aid). */
+int tsr_ctx_set_wait_budget(tsr_ctx* ctx, int64_t cycles);
 
 /* ---- Khatri-Rao: crates/tenrso-kernels/src/khatri_rao.rs:56-89 ----------
  * out (I*J x K) with row a*J + b = A[a,:] * B[b,:]. Host pointers. */
@@ -129,6 +135,17 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
                                const int64_t* shape, const float* const* d_factors, int64_t rank,
                                int mode, int precision, int iters, int flush_l2,
                                double* ms_per_launch, int64_t* splits_out);
+
+/* The FP64 inverse the CP-ALS solve applies (the step that replaces the
+ * per-row scirs2_linalg::lstsq of solve_least_squares, cp/helpers.rs:455-495,
+ * with the same ridge retry): `gram` (rank x rank, row-major, symmetric, host)
+ * is inverted `iters` times by the sweep's inverse kernel, the result copied
+ * to `inverse` (host), *ridge_used set to 0 (none), 1 (eps*rank*10) or 2
+ * (scaled by the mean diagonal), and *ms_per_launch to the mean device time
+ * of one launch (CUDA events, warm). TSR_E_NOT_SPD when every ridge fails.
+ * No tenrso counterpart (test and measurement aid). */
+int tsr_gram_inverse_f64(tsr_ctx* ctx, const double* gram, int64_t rank, int iters,
+                         double* inverse, int* ridge_used, double* ms_per_launch);
 
 /* Allocation-free MTTKRP of mode 0 (FP32 split-K path). No tenrso
  * counterpart: it exists for callers that cannot call cudaMalloc, such as a

@@ -12,6 +12,7 @@ from .dense import (  # noqa: F401
     cp_als,
     cp_als_dev,
     default_context,
+    gram_inverse,
     khatri_rao,
     mttkrp,
     mttkrp_all_modes,

@@ -50,12 +50,15 @@ SIGNATURES = {
     "tsr_ctx_destroy": (C.c_int, [P]),
     "tsr_ctx_synchronize": (C.c_int, [P]),
     "tsr_ctx_launch_count": (I64, [P]),
+    "tsr_ctx_set_wait_budget": (C.c_int, [P, I64]),
     "tsr_khatri_rao_f32": (C.c_int, [P, P, I64, I64, P, I64, I64, P]),
     "tsr_mttkrp_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, P]),
     "tsr_mttkrp_blocked_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, I64,
                                          C.c_int, P]),
     "tsr_mttkrp_all_modes_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, P]),
     "tsr_mttkrp_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, C.c_int, P]),
+    "tsr_gram_inverse_f64": (C.c_int, [P, P, I64, C.c_int, P, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_double)]),
     "tsr_profile_mttkrp_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.POINTER(C.c_double), PI64]),
     "tsr_mttkrp_mode0_noalloc_f32": (C.c_int, [P, P, C.c_int, P, P, I64, P]),

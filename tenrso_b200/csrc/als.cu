@@ -93,34 +93,46 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
   }
 }
 
-// Gauss-Jordan inverse of the (padded) Hadamard G as N uniform rank-1
-// updates, no pivoting.
+// Gauss-Jordan inverse of the (padded) Hadamard G in N/2 steps of 2 x 2
+// pivot blocks, no pivoting.
 //
 // G is first scaled to unit diagonal, G' = D G D with D = diag(1/sqrt(G_ii)),
-// so that G^-1 = D G'^-1 D and every pivot lies in (0, 1] (for an SPD matrix
-// the pivots are the LDL^T pivots, which never exceed the diagonal). One
-// Gauss-Jordan step k with pivot p is then exactly
-//   A <- A - u w^T,  u = column k of A except u_k = p - 1,
-//                    w = (row k of A except w_k = p + 1) / p,
-// which yields the pivot row A_kj / p, the pivot column -A_ik / p and the
-// corner 1 / p without special cases; with p <= 1 the +-1 terms do not cancel.
-// After steps 0..k-1 the matrix is symmetric within the processed and within
-// the unprocessed indices and antisymmetric across them, so column k is row k
-// with the sign of its processed entries flipped: u and w both follow from
-// row k alone.
+// so that G^-1 = D G'^-1 D. Step s eliminates the pivot pair K = {k, k+1},
+// k = 2s, with the 2 x 2 block P = A[K][K] (symmetric and, for an SPD G,
+// positive definite: its determinant is the product of two LDL^T pivots).
+// One step is exactly the uniform rank-2 update
+//   A <- A - U W^T,  U[i] = A[i][K]          (i not in K),  U[K] = P - I,
+//                    W[j] = P^-1 A[K][j]     (j not in K),  W[K] = I + P^-1,
+// which yields the pivot rows P^-1 A[K][j], the pivot columns -A[i][K] P^-1
+// and the corner P^-1 without special cases (block form of the scalar
+// identities u_k = p - 1, w_k = (p + 1) / p). P^-1 = adj(P) / det(P) costs one
+// reciprocal per step. After steps 0..s-1 the matrix is symmetric within the
+// processed and within the unprocessed indices and antisymmetric across them,
+// so U follows from the pivot rows with the sign of the processed entries
+// flipped: a step needs the two pivot rows only.
 //
-// Thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and columns tx + 16b
-// (RB x RB doubles in registers). The 16 owners of row k + 1 (one half-warp)
-// update that row first, form u and w of step k + 1 from it and publish them
-// into a double buffer, so a step costs every other thread 2 RB shared loads
-// and RB^2 FMAs, and one barrier. A pivot that is not positive, not finite or
-// below 1e-290 (a non-positive diagonal included) sets the "not SPD" flag,
-// read once after the last step.
+// Roles (kGjThreads = 288 threads):
+//   bulk warps 0..7   thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and
+//                     columns tx + 16b (RB x RB doubles in registers) and only
+//                     applies the published updates: per step 2 RB 16-byte
+//                     shared loads and 2 RB^2 FMAs. During step s the owners
+//                     of rows 2s+4 and 2s+5 also copy them, updated through
+//                     step s, into a staging buffer.
+//   pivot warp 8      the serial chain: at step s it takes rows 2s+2, 2s+3
+//                     (staged during step s-1), applies step s to them, forms
+//                     U and W of step s+1 and publishes them. It holds no
+//                     other row, so its chain is not queued behind the bulk
+//                     FMAs; one barrier per step.
+// A pivot that is not positive, not finite or below 1e-290 (a non-positive
+// diagonal included) sets the "not SPD" flag, read once after the last step.
+constexpr int kGjThreads = 288;
+
 template <int RB>
 struct GjShared {
-  double u[2][16 * RB];  // pivot column of the step, u_k = p - 1 (double buffered)
-  double w[2][16 * RB];  // pivot row of the step over p, w_k = (p + 1) / p
-  double dsc[16 * RB];   // the diagonal scaling 1 / sqrt(G_ii)
+  double2 u[2][16 * RB];        // [buffer][row]: (U[i][0], U[i][1]) of the step
+  double2 w[2][16 * RB];        // [buffer][column]: (W[j][0], W[j][1]) of the step
+  double stage[2][2][16 * RB];  // [slot][pivot row of the pair][column]
+  double dsc[16 * RB];          // the diagonal scaling 1 / sqrt(G_ii)
   double scale;
   int bad;
 };
@@ -136,96 +148,156 @@ __device__ __forceinline__ double recip_nr(double p) {
   return x;
 }
 
-// Called by the half-warp that owns row k (ty == k & 15), `row` holding its
-// step-k values A_kj for j = tx + 16 bj: publishes u and w of step k.
+// Called by the pivot warp holding rows k and k+1 (k even): lanes 0-15 hold
+// row k, lanes 16-31 row k+1, at columns tx + 16 bj (`row`, their values after
+// every earlier step). Publishes U and W of the step into buffer `buf`.
 template <int RB>
-__device__ __forceinline__ void gj_publish(const double (&row)[RB], int k, int tx, int buf,
-                                           GjShared<RB>& sh) {
-  const unsigned mask = 0xFFFFu << (threadIdx.x & 16);
-  const int kb = k >> 4;
+__device__ __forceinline__ void gj2_publish(const double (&row)[RB], int k, int buf,
+                                            GjShared<RB>& sh) {
+  const int lane = threadIdx.x & 31, tx = lane & 15, half = lane >> 4;
+  const int kb = k >> 4, kt = k & 15;  // columns k and k+1 are kt, kt+1 of block kb
+  // the partner row's values at this lane's columns (independent of the pivot)
+  double o[RB];
+#pragma unroll
+  for (int bj = 0; bj < RB; ++bj) o[bj] = __shfl_xor_sync(0xffffffffu, row[bj], 16);
   double mine = row[0];
 #pragma unroll
   for (int bj = 1; bj < RB; ++bj)
     if (bj == kb) mine = row[bj];
-  const double p = __shfl_sync(mask, mine, k & 15, 16);  // A_kk
-  const bool good = p >= 1e-290 && isfinite(p);
-  if (!good && tx == 0) sh.bad = 1;
-  const double inv = recip_nr(good ? p : 1.0);
+  const double a = __shfl_sync(0xffffffffu, mine, kt);           // A[k][k]
+  const double b = __shfl_sync(0xffffffffu, mine, kt + 1);       // A[k][k+1]
+  const double d = __shfl_sync(0xffffffffu, mine, 16 + kt + 1);  // A[k+1][k+1]
+  const double det = fma(a, d, -(b * b));
+  // LDL^T pivots a and det / a
+  const bool good = a >= 1e-290 && det >= 1e-290 * a && isfinite(a) && isfinite(det);
+  if (!good && lane == 0) sh.bad = 1;
+  const double id = recip_nr(good ? det : 1.0);
+  const double p00 = d * id, p01 = -b * id, p11 = a * id;  // P^-1 (symmetric)
 #pragma unroll
   for (int bj = 0; bj < RB; ++bj) {
     const int j = tx + 16 * bj;
     const double r = row[bj];
-    sh.w[buf][j] = (j == k ? p + 1.0 : r) * inv;
-    sh.u[buf][j] = j == k ? p - 1.0 : (j < k ? -r : r);
+    const double r0 = half ? o[bj] : r, r1 = half ? r : o[bj];
+    double w0 = fma(p00, r0, p01 * r1), w1 = fma(p01, r0, p11 * r1);
+    const double sg = j < k ? -1.0 : 1.0;
+    double u0 = sg * r0, u1 = sg * r1;
+    if (j == k) {
+      w0 = 1.0 + p00;
+      w1 = p01;
+      u0 = a - 1.0;
+      u1 = b;
+    } else if (j == k + 1) {
+      w0 = p01;
+      w1 = 1.0 + p11;
+      u0 = b;
+      u1 = d - 1.0;
+    }
+    // the two half-warps hold the same columns: one writes each pair
+    if (half == 0) {
+      sh.w[buf][j] = make_double2(w0, w1);
+      sh.u[buf][j] = make_double2(u0, u1);
+    }
   }
 }
 
+// Whole CTA (kGjThreads). `a` is meaningful in the bulk threads only.
 template <int RB>
 __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
   constexpr int N = 16 * RB;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  constexpr int STEPS = N / 2;
+  const bool bulk = threadIdx.x < 256;
+  const int tx = threadIdx.x & 15, ty = (threadIdx.x >> 4) & 15;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // diagonal scaling (a non-positive diagonal scales its row to zero, whose
   // pivot then reports "not SPD")
   if (threadIdx.x == 0) sh.bad = 0;
+  if (bulk) {
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj)
-      if (ty + 16 * ai == tx + 16 * bj) {
-        const double g = a[ai][bj];
-        sh.dsc[ty + 16 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
-      }
+      for (int bj = 0; bj < RB; ++bj)
+        if (ty + 16 * ai == tx + 16 * bj) {
+          const double g = a[ai][bj];
+          sh.dsc[ty + 16 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
+        }
+  }
   __syncthreads();
   double di[RB], dj[RB];
 #pragma unroll
   for (int ai = 0; ai < RB; ++ai) di[ai] = sh.dsc[ty + 16 * ai];
 #pragma unroll
   for (int bj = 0; bj < RB; ++bj) dj[bj] = sh.dsc[tx + 16 * bj];
-#pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
-#pragma unroll
-    for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
-  if (ty == 0) gj_publish<RB>(a[0], 0, tx, 0, sh);
-  __syncthreads();
-#pragma unroll 1
-  for (int k = 0; k < N; ++k) {
-    const int buf = k & 1;
-    double u[RB], w[RB];
-#pragma unroll
-    for (int ai = 0; ai < RB; ++ai) u[ai] = sh.u[buf][ty + 16 * ai];
-#pragma unroll
-    for (int bj = 0; bj < RB; ++bj) w[bj] = sh.w[buf][tx + 16 * bj];
-    const int k1 = k + 1;
-    if (k1 < N && ty == (k1 & 15)) {
-      // row k + 1 first: its step-(k+1) u and w are the critical path. The
-      // row is picked by selects (static register indices only).
-      const int kb1 = k1 >> 4;
-      double row[RB], uk = u[0];
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj) row[bj] = a[0][bj];
-#pragma unroll
-      for (int ai = 1; ai < RB; ++ai) {
-        const bool sel = ai == kb1;
-        uk = sel ? u[ai] : uk;
-#pragma unroll
-        for (int bj = 0; bj < RB; ++bj) row[bj] = sel ? a[ai][bj] : row[bj];
-      }
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj) row[bj] = fma(-uk, w[bj], row[bj]);
-      gj_publish<RB>(row, k1, tx, buf ^ 1, sh);
-    }
+  if (bulk) {
 #pragma unroll
     for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) a[ai][bj] = fma(-u[ai], w[bj], a[ai][bj]);
+      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
+    // rows 0, 1 (step 0's pivots) into slot 0 and rows 2, 3 into slot 1
+    if (warp <= 1) {
+      const int h = ty & 1;
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) sh.stage[warp][h][tx + 16 * bj] = a[0][bj];
+    }
+  }
+  __syncthreads();
+  double prow[RB];  // pivot warp: its two rows (lanes 0-15 first, 16-31 second)
+  if (!bulk) {
+    const int h = lane >> 4;
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) prow[bj] = sh.stage[0][h][tx + 16 * bj];
+    gj2_publish<RB>(prow, 0, 0, sh);
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 0; s < STEPS; ++s) {
+    const int buf = s & 1, k = 2 * s;
+    if (bulk) {
+      double2 u[RB], w[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) u[ai] = sh.u[buf][ty + 16 * ai];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) w[bj] = sh.w[buf][tx + 16 * bj];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj)
+          a[ai][bj] = fma(-u[ai].x, w[bj].x, fma(-u[ai].y, w[bj].y, a[ai][bj]));
+      // rows k+4, k+5 (step s+2's pivots), updated through step s, to the
+      // pivot warp: staged in slot s & 1
+      const int k4 = k + 4;
+      if (k4 < N && warp == ((k4 & 15) >> 1)) {
+        const int kb4 = k4 >> 4, h = ty & 1;
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) {
+          double v = a[0][bj];
+#pragma unroll
+          for (int ai = 1; ai < RB; ++ai)
+            if (ai == kb4) v = a[ai][bj];
+          sh.stage[buf][h][tx + 16 * bj] = v;
+        }
+      }
+    } else if (s + 1 < STEPS) {
+      // rows k+2, k+3 as of step s-1 (staged during step s-1, slot (s+1) & 1),
+      // step s applied, then step s+1 published
+      const int h = lane >> 4, k2 = k + 2;
+      const double2 ur = sh.u[buf][k2 + h];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) {
+        const double2 wv = sh.w[buf][tx + 16 * bj];
+        prow[bj] = fma(-ur.x, wv.x, fma(-ur.y, wv.y, sh.stage[buf ^ 1][h][tx + 16 * bj]));
+      }
+      gj2_publish<RB>(prow, k2, buf ^ 1, sh);
+    }
     __syncthreads();
   }
   if (sh.bad) return false;
   // G^-1 = D G'^-1 D
+  if (bulk) {
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
+      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
+  }
   return true;
 }
 
@@ -345,7 +417,7 @@ __global__ void fit_kernel(AlsBuffers b, double tol) {
 // solve_least_squares does, helpers.rs:477-490); zeroes this mode's Gram
 // accumulator (and <X,Xhat> for the last mode) for the solve that follows.
 template <int RB>
-__global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
+__global__ void __launch_bounds__(kGjThreads) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
                                                    float ridge_eps, int last, double tol,
                                                    double l2) {
   __shared__ GjShared<RB> gsh;
@@ -358,16 +430,23 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
     if (*(volatile int*)&st->done) return;
   }
   const int RR = R * R;
+  // threads 0..255 hold the matrix, 16 x 16 grid (RB x RB each); warp 8 is
+  // the inverse's pivot warp
+  const bool bulk = threadIdx.x < 256;
   double a[RB][RB];
-  load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
-  if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+  if (bulk) {
+    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
+    if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+  }
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
   bool ok = gj_inverse<RB>(a, gsh);
   if (!ok) {
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
-    if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+    if (bulk) {
+      load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
+      if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+    }
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
   }
@@ -386,9 +465,11 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
       if (threadIdx.x == 0) gsh.scale = d / R;
     }
     __syncthreads();
-    load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps * fmax(gsh.scale, 1.0),
-                      a, false);
-    if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+    if (bulk) {
+      load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R,
+                        (double)ridge_eps * fmax(gsh.scale, 1.0), a, false);
+      if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+    }
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 2;
   }
@@ -400,13 +481,15 @@ __global__ void __launch_bounds__(256) chol_kernel(AlsBuffers b, int ndim, int m
     return;
   }
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  if (bulk) {
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) {
-      const int i = ty + 16 * ai, j = tx + 16 * bj;
-      if (i < R && j < R) b.ginv[i * R + j] = a[ai][bj];
-    }
+      for (int bj = 0; bj < RB; ++bj) {
+        const int i = ty + 16 * ai, j = tx + 16 * bj;
+        if (i < R && j < R) b.ginv[i * R + j] = a[ai][bj];
+      }
+  }
   double* gm = b.grams + (int64_t)mode * RR;
   for (int e = threadIdx.x; e < RR; e += blockDim.x) gm[e] = 0.0;
   if (last && threadIdx.x == 0) {
@@ -445,7 +528,7 @@ template <int RB>
 __global__ void __launch_bounds__(256)
 solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
              int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
-             double tol, float l1, int nonneg) {
+             double tol, float l1, int nonneg, uint8_t* __restrict__ bimg, int img_n_pad) {
   extern __shared__ __align__(16) double sh[];
   __shared__ __align__(8) uint64_t gi_bar;
   __shared__ int gi_state;  // 0 copy in flight, 1 landed, 2 gave up
@@ -590,6 +673,19 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
       if (l1 > 0.f) v = v > l1 ? v - l1 : (v < -l1 ? v + l1 : 0.f);
       if (nonneg) v = fmaxf(v, 0.f);
       U[(r0 + i) * R + c] = v;
+      if (bimg) {
+        // the new entry's bf16 hi/lo halves into the next MTTKRP's B image:
+        // k-block k >> 6, rows c (hi) and img_n_pad + c (lo), 16-byte chunk
+        // (k & 63) >> 3 at its 128-byte-swizzled position, element k & 7
+        const int64_t k = r0 + i;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+        uint8_t* tile = bimg + (size_t)(k >> 6) * 2 * img_n_pad * 128;
+        const int cq = (int)((k & 63) >> 3), el = (int)(k & 7) * 2;
+        const int rh = c, rl = img_n_pad + c;
+        *reinterpret_cast<__nv_bfloat16*>(tile + rh * 128 + ((cq ^ (rh & 7)) << 4) + el) = h;
+        *reinterpret_cast<__nv_bfloat16*>(tile + rl * 128 + ((cq ^ (rl & 7)) << 4) + el) = l;
+      }
       Us[e] = (double)v;
       ip += Ms[e] * (double)v;
     }
@@ -704,13 +800,13 @@ int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const int lst = last ? 1 : 0;
   switch ((R + 15) / 16) {
-    case 1: chol_kernel<1><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 2: chol_kernel<2><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 3: chol_kernel<3><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 4: chol_kernel<4><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 5: chol_kernel<5><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 6: chol_kernel<6><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    default: chol_kernel<7><<<1, 256, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 1: chol_kernel<1><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 2: chol_kernel<2><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 3: chol_kernel<3><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 4: chol_kernel<4><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 5: chol_kernel<5><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 6: chol_kernel<6><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    default: chol_kernel<7><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
   }
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
@@ -744,7 +840,7 @@ int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int 
 
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
-                 double tol, float l1, int nonneg) {
+                 double tol, float l1, int nonneg, uint8_t* bimg, int img_n_pad) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   // about 64 row chunks (one per CTA) for small modes, so that the Gram
   // atomics stay few; 16-row chunks grid-strided over at most 8 CTAs per SM
@@ -759,7 +855,7 @@ int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float*
   const int lst = last ? 1 : 0;
 #define TSR_SOLVE(RB)                                                                    \
   TSR_CUDA(launch_pdl(solve_kernel<RB>, dim3(grid), dim3(256), smem, s, b, partials, splits, \
-                      rows, R, rpc, U, gram, lst, ndim, tol, l1, nonneg))
+                      rows, R, rpc, U, gram, lst, ndim, tol, l1, nonneg, bimg, img_n_pad))
   switch ((R + 15) / 16) {
     case 1: TSR_SOLVE(1); break;
     case 2: TSR_SOLVE(2); break;

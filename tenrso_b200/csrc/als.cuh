@@ -87,8 +87,11 @@ int launch_fit(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int 
 // and marks the sweep's fit pending. Each new fp32 entry is soft-thresholded
 // by l1 when l1 > 0 and clamped at zero when nonneg (core.rs:350-359) before
 // it is stored and enters the Gram and the fit.
+// With bimg set, each new entry's bf16 hi/lo halves are also written into that
+// B image (mttkrp3.cu layout, n_pad img_n_pad) for the next MTTKRP.
 int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float* partials,
                  int splits, int64_t rows, int R, float* U, double* gram, bool last, int ndim,
-                 double tol, float l1 = 0.f, int nonneg = 0);
+                 double tol, float l1 = 0.f, int nonneg = 0, uint8_t* bimg = nullptr,
+                 int img_n_pad = 0);
 
 }  // namespace tsr

@@ -70,6 +70,9 @@ enum Slot {
   SLOT_MISC1,
   SLOT_MISC2,
   SLOT_MISC3,
+  SLOT_D3_HI,         // 3-way single-layout path: bf16 hi half of X
+  SLOT_D3_LO,         //   bf16 lo half of X
+  SLOT_D3_IMG,        //   B images of the contracted factors
   SLOT_SPARSE0,
   SLOT_SPARSE1 = SLOT_SPARSE0 + 16,
   SLOT_COUNT = SLOT_SPARSE1 + 16
@@ -88,6 +91,10 @@ struct tsr_ctx {
   size_t pinned_bytes = 0;
   unsigned* d_status = nullptr;  // device status word
   int64_t launches = 0;          // kernels launched by this context (counter)
+  // clock-cycle budget of each bounded pipeline wait in the tensor-core
+  // MTTKRP (about 1 s by default; tsr_ctx_set_wait_budget lowers it to test
+  // the timeout path)
+  long long wait_budget = 1ll << 31;
   // SMs the MTTKRP grids leave free so that the side-stream FP64 kernels of
   // the ALS sweep (Gram, inverse, fit) run concurrently instead of queueing
   int reserve_sms = 8;
@@ -118,6 +125,9 @@ int read_status(tsr_ctx* ctx, unsigned* out);  // synchronizes the stream
 // Evict L2 by reading a buffer of twice its size (clean lines only).
 int flush_l2(tsr_ctx* ctx, cudaStream_t s);
 int reset_status(tsr_ctx* ctx);
+// Synchronizes, reads and clears the status word: TSR_E_TIMEOUT when a
+// kernel's bounded wait gave up, else TSR_OK.
+int check_device_status(tsr_ctx* ctx);
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }

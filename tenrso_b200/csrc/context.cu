@@ -107,6 +107,15 @@ int reset_status(tsr_ctx* ctx) {
   return TSR_OK;
 }
 
+int check_device_status(tsr_ctx* ctx) {
+  unsigned st = 0;
+  TSR_TRY(read_status(ctx, &st));
+  if (st) TSR_TRY(reset_status(ctx));
+  if (st & DS_TIMEOUT)
+    return fail(TSR_E_TIMEOUT, "device wait timed out in the MTTKRP kernel");
+  return TSR_OK;
+}
+
 Unfolding make_unfolding(int ndim, const int64_t* shape, int mode) {
   Unfolding u{};
   u.ndim = ndim;
@@ -432,5 +441,11 @@ int tsr_ctx_synchronize(tsr_ctx* ctx) {
 }
 
 int64_t tsr_ctx_launch_count(const tsr_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int tsr_ctx_set_wait_budget(tsr_ctx* ctx, int64_t cycles) {
+  TSR_TRY(check_ctx(ctx));
+  ctx->wait_budget = cycles > 0 ? (long long)cycles : (1ll << 31);
+  return TSR_OK;
+}
 
 }  // extern "C"

@@ -200,9 +200,52 @@ int check_precision(int precision) {
   return TSR_OK;
 }
 
+// The single-layout BF16x3 operand of a 3-way tensor for a standalone MTTKRP
+// of `mode`: X's hi/lo halves and the B image of the contracted factor (U1
+// for mode 2, U2 otherwise), in the context's slots.
+static bool dense3_usable(int ndim, const int64_t* shape, int R, int precision, const float* dX) {
+  return precision == TSR_PREC_BF16X3 && dense3_supported(ndim, shape, R) &&
+         ((uintptr_t)dX & 15) == 0;
+}
+
+static int prepare_dense3(tsr_ctx* ctx, const float* dX, const int64_t* shape, int R,
+                          const FactorTable& ft, int mode, Dense3* d) {
+  std::memset(d, 0, sizeof(*d));
+  d->I = shape[0];
+  d->J = shape[1];
+  d->K = shape[2];
+  d->R = R;
+  d->n_pad = dense3_n_pad(R);
+  const size_t n = (size_t)(d->I * d->J * d->K);
+  void *hp, *lp, *ip, *np;
+  TSR_TRY(slot_get(ctx, SLOT_D3_HI, sizeof(__nv_bfloat16) * n, &hp));
+  TSR_TRY(slot_get(ctx, SLOT_D3_LO, sizeof(__nv_bfloat16) * n, &lp));
+  const int c = mode == 2 ? 1 : 2;
+  const int64_t L = c == 1 ? d->J : d->K;
+  TSR_TRY(slot_get(ctx, SLOT_D3_IMG, bimage_bytes(L, d->n_pad), &ip));
+  TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(double), &np));  // ||X||^2, not needed here
+  d->hi = (const __nv_bfloat16*)hp;
+  d->lo = (const __nv_bfloat16*)lp;
+  d->bimg[c] = (uint8_t*)ip;
+  TSR_TRY(launch_split_bf16(ctx, ctx->stream, dX, (int64_t)n, (__nv_bfloat16*)hp,
+                            (__nv_bfloat16*)lp, (double*)np));
+  TSR_TRY(launch_bimage(ctx, ctx->stream, ft.ptr[c], L, R, d->n_pad, d->bimg[c]));
+  return TSR_OK;
+}
+
 // Device MTTKRP for one mode into d_out (I_mode x R).
 int mttkrp_device(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape,
                   const FactorTable& ft, int R, int mode, int precision, float* d_out) {
+  if (dense3_usable(ndim, shape, R, precision, dX)) {
+    Dense3 d;
+    TSR_TRY(prepare_dense3(ctx, dX, shape, R, ft, mode, &d));
+    const SplitPlan plan = plan_mttkrp3(ctx, d, mode);
+    void* p;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS,
+                     sizeof(float) * (size_t)plan.splits * dense3_rows(d, mode) * R, &p));
+    TSR_TRY(launch_mttkrp3(ctx, ctx->stream, d, mode, ft, plan, (float*)p, false));
+    return launch_mttkrp_reduce(ctx, (float*)p, plan.splits, shape[mode] * R, d_out);
+  }
   ModeOperand op;
   TSR_TRY(prepare_mode(ctx, dX, ndim, shape, mode, precision, 0, &op));
   float* partials;
@@ -241,6 +284,9 @@ struct SweepArgs {
   AlsBuffers b;
   const tsr_sparse* sp;  // sparse source (CSF MTTKRP) instead of the dense unfoldings
   double* acc64;         // sparse: FP64 accumulator of the CSF MTTKRP
+  int d3_on;             // 3-way BF16x3: the single-layout MTTKRP on d3
+  Dense3 d3;
+  long long wait_budget;  // baked into the captured MTTKRP launches
 };
 
 static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<ModeOperand>& ops) {
@@ -253,14 +299,21 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
     TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
     float* partials = a.partials;
     int splits = 1;
-    if (a.sp)
+    uint8_t* img = nullptr;  // the B image this mode's new factor feeds
+    if (a.sp) {
       TSR_TRY(launch_mttkrp_csf(ctx, A, a.sp, a.ft, a.R, n, partials, a.acc64));
-    else
+    } else if (a.d3_on) {
+      const SplitPlan plan = plan_mttkrp3(ctx, a.d3, n);
+      TSR_TRY(launch_mttkrp3(ctx, A, a.d3, n, a.ft, plan, partials, true));
+      splits = plan.splits;
+      img = n == 0 ? nullptr : a.d3.bimg[n];  // U1 feeds mode 2, U2 modes 0 and 1
+    } else {
       TSR_TRY(run_mttkrp_partials(ctx, ops[n], a.ft, a.R, a.precision, &partials, &splits));
+    }
     TSR_CUDA(cudaStreamWaitEvent(A, ctx->ev[1 + 2 * n], 0));
     TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
                          const_cast<float*>(a.ft.ptr[n]), a.b.grams + (size_t)n * a.R * a.R,
-                         last, a.ndim, a.tol, a.l1, a.nonneg));
+                         last, a.ndim, a.tol, a.l1, a.nonneg, img, a.d3.n_pad));
     if (!last) {  // the next inverse needs this mode's Gram
       TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
       TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
@@ -309,6 +362,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   a.tol = tol;
   a.ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
   a.sp = sp;
+  a.wait_budget = ctx->wait_budget;
   if (cons) {
     a.l2 = cons->l2;
     a.l1 = (float)cons->l1;  // the threshold in the factors' type (core.rs:351)
@@ -340,6 +394,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   a.b.history = (double*)((char*)stp + 256);
   TSR_CUDA(cudaMemsetAsync(stp, 0, sbytes, ctx->stream));
   TSR_CUDA(cudaMemsetAsync(gp, 0, gbytes, ctx->stream));
+  TSR_TRY(reset_status(ctx));  // the MTTKRP kernels' status word
   if (cons && cons->nonnegative && cons->validate_nonneg_input) {
     // helpers.rs:705-716: one pass over X before any factor is touched
     TSR_TRY(launch_any_negative(ctx, ctx->stream, dX, n, &a.b.state->pad));
@@ -357,8 +412,49 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   // in every mttkrp call, mttkrp.rs:126)
   std::vector<ModeOperand> ops(ndim);
   size_t pmax = 0;
-  const bool fused_unfold = !sp && max_iters > 0 && unfold3_supported(ndim, shape);
-  if (max_iters > 0 && sp) {
+  // 3-way BF16x3: one bf16 hi/lo copy of X read by every mode (no unfoldings)
+  const bool d3 = !sp && max_iters > 0 && precision == TSR_PREC_BF16X3 &&
+                  dense3_supported(ndim, shape, R) && ((uintptr_t)dX & 15) == 0;
+  const bool fused_unfold = !d3 && !sp && max_iters > 0 && unfold3_supported(ndim, shape);
+  if (d3) {
+    Dense3& d = a.d3;
+    a.d3_on = 1;
+    d.I = shape[0];
+    d.J = shape[1];
+    d.K = shape[2];
+    d.R = R;
+    d.n_pad = dense3_n_pad(R);
+    void *hp, *lp, *ip;
+    TSR_TRY(slot_get(ctx, SLOT_D3_HI, sizeof(__nv_bfloat16) * (size_t)n, &hp));
+    TSR_TRY(slot_get(ctx, SLOT_D3_LO, sizeof(__nv_bfloat16) * (size_t)n, &lp));
+    const size_t img1 = bimage_bytes(d.J, d.n_pad), img2 = bimage_bytes(d.K, d.n_pad);
+    TSR_TRY(slot_get(ctx, SLOT_D3_IMG, img1 + img2, &ip));
+    d.hi = (const __nv_bfloat16*)hp;
+    d.lo = (const __nv_bfloat16*)lp;
+    d.bimg[0] = nullptr;
+    d.bimg[1] = (uint8_t*)ip;
+    d.bimg[2] = (uint8_t*)ip + img1;
+    for (int m = 0; m < 3; ++m) {
+      const SplitPlan p = plan_mttkrp3(ctx, d, m);
+      pmax = std::max(pmax, (size_t)p.splits * dense3_rows(d, m) * R);
+    }
+    void* pp;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
+    a.partials = (float*)pp;
+    // the initial Grams on the aux stream beside the split pass; the B images
+    // of the initial U1 and U2 (the solves rewrite them as the factors change)
+    TSR_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    TSR_CUDA(cudaStreamWaitEvent(ctx->aux, ctx->ev[0], 0));
+    for (int m = 0; m < ndim; ++m)
+      TSR_TRY(launch_gram(ctx, ctx->aux, a.ft.ptr[m], shape[m], R,
+                          a.b.grams + (size_t)m * R * R, false));
+    TSR_TRY(launch_bimage(ctx, ctx->aux, a.ft.ptr[1], d.J, R, d.n_pad, d.bimg[1]));
+    TSR_TRY(launch_bimage(ctx, ctx->aux, a.ft.ptr[2], d.K, R, d.n_pad, d.bimg[2]));
+    TSR_CUDA(cudaEventRecord(ctx->ev[1], ctx->aux));
+    TSR_TRY(launch_split_bf16(ctx, ctx->stream, dX, n, (__nv_bfloat16*)hp, (__nv_bfloat16*)lp,
+                              &a.b.state->xnorm_sq));
+    TSR_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev[1], 0));
+  } else if (max_iters > 0 && sp) {
     for (int m = 0; m < ndim; ++m) pmax = std::max(pmax, (size_t)shape[m] * R);
     void* pp;
     TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
@@ -415,9 +511,9 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   if (sp)  // sum of squared values, FP64, computed when the tensor was built
     TSR_CUDA(cudaMemcpyAsync(&a.b.state->xnorm_sq, &sp->norm_sq, sizeof(double),
                              cudaMemcpyHostToDevice, ctx->stream));
-  else if (!fused_unfold)
+  else if (!fused_unfold && !d3)
     TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, &a.b.state->xnorm_sq));
-  if (!fused_unfold)
+  if (!fused_unfold && !d3)
     for (int m = 0; m < ndim; ++m)
       TSR_TRY(launch_gram(ctx, ctx->stream, a.ft.ptr[m], shape[m], R,
                           a.b.grams + (size_t)m * R * R, false));
@@ -499,7 +595,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   if (max_iters > 0) TSR_TRY(launch_fit(ctx, ctx->stream, a.b, ndim, R, tol));
   AlsState hs;
   TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
-  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSR_TRY(check_device_status(ctx));  // synchronizes; a timed-out MTTKRP wait
   if (hs.status & DS_TIMEOUT)
     return fail(TSR_E_TIMEOUT, "device wait timed out in the CP-ALS sweep");
   if (hs.status & DS_NOT_SPD)
@@ -535,6 +631,7 @@ void init_kernel_attributes() {
   std::lock_guard<std::mutex> lock(mu);
   if (done_mask & (1ull << dev)) return;
   init_tc_attributes();
+  init_mttkrp3_attributes();
   init_simt_attributes();
   init_als_attributes();
   init_adjoint_attributes();
@@ -595,8 +692,7 @@ int tsr_mttkrp_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* s
   TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * nout, &dout));
   TSR_TRY(mttkrp_device(ctx, dX, ndim, shape, ft, R, mode, precision, (float*)dout));
   TSR_CUDA(cudaMemcpyAsync(out, dout, sizeof(float) * nout, cudaMemcpyDeviceToHost, ctx->stream));
-  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
-  return TSR_OK;
+  return check_device_status(ctx);
 }
 
 int tsr_mttkrp_blocked_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
@@ -627,7 +723,7 @@ int tsr_mttkrp_all_modes_f32(tsr_ctx* ctx, const float* tensor, int ndim, const 
     TSR_TRY(mttkrp_device(ctx, dX, ndim, shape, ft, R, m, precision, (float*)dout));
     TSR_CUDA(cudaMemcpyAsync(out[m], dout, sizeof(float) * shape[m] * R, cudaMemcpyDeviceToHost,
                              ctx->stream));
-    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+    TSR_TRY(check_device_status(ctx));
   }
   return TSR_OK;
 }
@@ -652,7 +748,9 @@ int tsr_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
     ft.ptr[m] = d_factors[m];
     ft.rows[m] = shape[m];
   }
-  return mttkrp_device(ctx, d_tensor, ndim, shape, ft, (int)rank, mode, precision, d_out);
+  TSR_TRY(mttkrp_device(ctx, d_tensor, ndim, shape, ft, (int)rank, mode, precision, d_out));
+  // a bounded wait that gave up is reported (this synchronizes the stream)
+  return check_device_status(ctx);
 }
 
 int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
@@ -670,8 +768,21 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
     ft.ptr[m] = d_factors[m];
     ft.rows[m] = shape[m];
   }
+  const bool d3 = dense3_usable(ndim, shape, (int)rank, precision, d_tensor);
   ModeOperand op;
-  TSR_TRY(prepare_mode(ctx, d_tensor, ndim, shape, mode, precision, 0, &op));
+  Dense3 d;
+  SplitPlan plan3;
+  float* partials3 = nullptr;
+  if (d3) {
+    TSR_TRY(prepare_dense3(ctx, d_tensor, shape, (int)rank, ft, mode, &d));
+    plan3 = plan_mttkrp3(ctx, d, mode);
+    void* p;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS,
+                     sizeof(float) * (size_t)plan3.splits * dense3_rows(d, mode) * rank, &p));
+    partials3 = (float*)p;
+  } else {
+    TSR_TRY(prepare_mode(ctx, d_tensor, ndim, shape, mode, precision, 0, &op));
+  }
   cudaEvent_t a, b;
   TSR_CUDA(cudaEventCreate(&a));
   TSR_CUDA(cudaEventCreate(&b));
@@ -681,7 +792,12 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
     if (flush_l2) TSR_TRY(::tsr::flush_l2(ctx, ctx->stream));
     float* partials;
     TSR_CUDA(cudaEventRecord(a, ctx->stream));
-    TSR_TRY(run_mttkrp_partials(ctx, op, ft, (int)rank, precision, &partials, &splits));
+    if (d3) {
+      TSR_TRY(launch_mttkrp3(ctx, ctx->stream, d, mode, ft, plan3, partials3, true));
+      splits = plan3.splits;
+    } else {
+      TSR_TRY(run_mttkrp_partials(ctx, op, ft, (int)rank, precision, &partials, &splits));
+    }
     TSR_CUDA(cudaEventRecord(b, ctx->stream));
     TSR_CUDA(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -692,6 +808,55 @@ int tsr_profile_mttkrp_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
   cudaEventDestroy(b);
   *ms_per_launch = total / iters;
   if (splits_out) *splits_out = splits;
+  return check_device_status(ctx);
+}
+
+int tsr_gram_inverse_f64(tsr_ctx* ctx, const double* gram, int64_t rank, int iters,
+                         double* inverse, int* ridge_used, double* ms_per_launch) {
+  if (!gram || !inverse || iters < 1) return fail(TSR_E_INVALID_ARG, "invalid argument");
+  if (rank < 1 || rank > kMaxRank)
+    return fail(TSR_E_UNSUPPORTED, "rank %lld outside 1..%d", (long long)rank, kMaxRank);
+  TSR_TRY(check_ctx(ctx));
+  const int R = (int)rank;
+  const size_t RR = (size_t)R * R;
+  // a 2-mode ALS state: Gram_0 = G, and the inverse of mode 1 is that of the
+  // Hadamard of the other Grams, i.e. of G itself
+  void *gp, *stp;
+  TSR_TRY(slot_get(ctx, SLOT_GRAMS, sizeof(double) * 5 * RR, &gp));
+  TSR_TRY(slot_get(ctx, SLOT_STATE, 256 + sizeof(double), &stp));
+  AlsBuffers b;
+  b.grams = (double*)gp;
+  b.hadam = b.grams + 2 * RR;
+  b.ginv = b.hadam + 2 * RR;
+  b.state = (AlsState*)stp;
+  b.history = (double*)((char*)stp + 256);
+  TSR_CUDA(cudaMemsetAsync(stp, 0, 256 + sizeof(double), ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(b.grams, gram, sizeof(double) * RR, cudaMemcpyHostToDevice,
+                           ctx->stream));
+  const float ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
+  cudaEvent_t e0, e1;
+  TSR_CUDA(cudaEventCreate(&e0));
+  TSR_CUDA(cudaEventCreate(&e1));
+  TSR_TRY(launch_chol(ctx, ctx->stream, b, 2, 1, R, ridge, false, 0.0));  // warm-up
+  TSR_CUDA(cudaEventRecord(e0, ctx->stream));
+  for (int i = 0; i < iters; ++i) TSR_TRY(launch_chol(ctx, ctx->stream, b, 2, 1, R, ridge, false, 0.0));
+  TSR_CUDA(cudaEventRecord(e1, ctx->stream));
+  AlsState hs;
+  TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(inverse, b.ginv, sizeof(double) * RR, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms_per_launch) *ms_per_launch = ms / iters;
+  if (ridge_used) *ridge_used = hs.ridge_used;
+  if (hs.status & DS_NOT_SPD)
+    return fail(TSR_E_NOT_SPD,
+                "Linear algebra error: Gram matrix is not positive definite (ridge %g also "
+                "failed)",
+                (double)ridge);
   return TSR_OK;
 }
 

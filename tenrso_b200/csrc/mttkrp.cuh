@@ -33,6 +33,33 @@ int launch_mttkrp_tc(tsr_ctx* ctx, const __nv_bfloat16* hi, const __nv_bfloat16*
                      const Unfolding& u, const KRSpec& kr, const SplitPlan& plan,
                      float* partials, bool a_resident = false);
 
+// Single-layout BF16x3 MTTKRP of a 3-way tensor (mttkrp3.cu): X split once
+// into bf16 hi/lo halves in its own row-major layout, read by every mode;
+// the contracted factor comes as a prebuilt swizzled "B image".
+struct Dense3 {
+  int64_t I, J, K;
+  int R, n_pad;  // n_pad: 32 (R <= 32) or 64
+  const __nv_bfloat16* hi;
+  const __nv_bfloat16* lo;
+  uint8_t* bimg[3];  // [1]: image of U1 (L = J, mode 2), [2]: of U2 (L = K, modes 0 and 1)
+};
+void init_mttkrp3_attributes();
+bool dense3_supported(int ndim, const int64_t* shape, int R);
+int dense3_n_pad(int R);
+size_t bimage_bytes(int64_t L, int n_pad);
+int64_t dense3_rows(const Dense3& d, int mode);
+// X (n floats, n % 4 == 0) -> hi / lo; ||X||^2 (FP64) added into *norm_sq.
+int launch_split_bf16(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, __nv_bfloat16* hi,
+                      __nv_bfloat16* lo, double* norm_sq);
+// The whole B image of U (L x R), zero padding included.
+int launch_bimage(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t L, int R, int n_pad,
+                  uint8_t* img);
+// SplitPlan: splits, k_per_split = runs per split, run_length = contracted length.
+SplitPlan plan_mttkrp3(const tsr_ctx* ctx, const Dense3& d, int mode);
+// Partials [splits][rows][R] of mode `mode`; the weights come from ft.
+int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, const FactorTable& ft,
+                   const SplitPlan& plan, float* partials, bool a_resident);
+
 // Materialised two-factor Khatri-Rao product (the public khatri_rao API).
 int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, int64_t J,
                       int64_t K, float* C);

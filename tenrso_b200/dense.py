@@ -39,6 +39,11 @@ class Context:
     def launches(self) -> int:
         return int(self._lib.tsr_ctx_launch_count(self.handle))
 
+    def set_wait_budget(self, cycles: int = 0):
+        """Budget (clock cycles) of each bounded wait in the tensor-core MTTKRP;
+        0 restores the default (about one second)."""
+        check(self._lib.tsr_ctx_set_wait_budget(self.handle, int(cycles)))
+
     def close(self):
         if self.handle:
             self._lib.tsr_ctx_destroy(self.handle)
@@ -287,3 +292,20 @@ def profile_mttkrp_dev(d_tensor: int, shape, d_factors: Sequence[int], rank: int
                                                  _prec(precision), iters, int(flush_l2),
                                                  C.byref(ms), C.byref(splits)))
     return ms.value, splits.value
+
+
+def gram_inverse(G: np.ndarray, iters: int = 1, ctx: Optional[Context] = None):
+    """The CP-ALS solve's FP64 inverse of a symmetric positive definite R x R
+    matrix (the stand-in for solve_least_squares' lstsq, cp/helpers.rs:455-495,
+    ridge retry included), run `iters` times on the device. Returns
+    (G^-1, ridge_used, mean ms per launch)."""
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    R = G.shape[0]
+    if G.shape != (R, R):
+        raise ValueError("gram_inverse needs a square matrix")
+    out = np.zeros_like(G)
+    ridge = C.c_int(0)
+    ms = C.c_double(0)
+    check(_lib.load().tsr_gram_inverse_f64(_ctx_handle(ctx), _ptr(G), R, int(iters), _ptr(out),
+                                           C.byref(ridge), C.byref(ms)))
+    return out, int(ridge.value), ms.value

@@ -111,6 +111,38 @@ def test_mttkrp_run_scaled_path(orc, shape, R):
         assert e <= 1e-4, (shape, R, mode, e)
 
 
+# 3-way tensors whose last mode is a multiple of 8 (middle and last modes at
+# most 384) take the single-layout tensor-core path: one bf16 hi/lo copy of X
+# read by every mode (modes 0 and 1 K-major, mode 2 MN-major), the contracted
+# factor as a prebuilt B image. These cover partial 128-row tiles in every
+# mode (mode 2's rows are the last mode: 136 ends inside a second 64-wide
+# box, 40 inside the first), contracted lengths that are not multiples of 64
+# (zero-filled boxes), middle modes that are not multiples of 8, ranks 1-64
+# (n_pad 32 and 64), single runs and the largest supported L.
+SINGLE_LAYOUT_SHAPES = [
+    ((37, 50, 72), 33),
+    ((5, 300, 16), 64),
+    ((129, 128, 136), 48),
+    ((64, 384, 384), 64),
+    ((20, 13, 40), 7),
+    ((1, 1, 8), 1),
+    ((300, 3, 24), 32),
+    ((17, 260, 200), 31),
+]
+
+
+@pytest.mark.parametrize("shape,R", SINGLE_LAYOUT_SHAPES)
+def test_mttkrp_single_layout_path(orc, shape, R):
+    X, fs = rand_problem(shape, R, seed=hash((shape, R)) & 0xFFFF, dist="normal")
+    X64 = X.astype(np.float64)
+    f64 = [f.astype(np.float64) for f in fs]
+    for mode in range(3):
+        out = tb.mttkrp(X, fs, mode, precision="bf16x3")
+        ref = orc.mttkrp(X64, f64, mode)
+        e = rel_err(out, ref)
+        assert e <= 1e-4, (shape, R, mode, e)
+
+
 @pytest.mark.parametrize("precision,tol", [("fp32", 1e-5), ("bf16x3", 1e-4)])
 def test_mttkrp_signed_data(orc, precision, tol):
     X, fs = rand_problem((48, 40, 36), 16, seed=3, dist="normal")
