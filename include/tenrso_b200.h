@@ -95,6 +95,16 @@ int64_t tsr_ctx_launch_count(const tsr_ctx* ctx);
  * return; the call then fails with TSR_E_TIMEOUT and the context stays usable.
  * No tenrso counterpart (failure-path testing aid). */
 int tsr_ctx_set_wait_budget(tsr_ctx* ctx, int64_t cycles);
+/* Kernel timeline tracing of the CP-ALS sweep (measurement aid, no tenrso
+ * counterpart). capacity > 0 allocates that many slots and turns tracing on
+ * (0 turns it off); while on, every dense cp_als call is captured afresh and
+ * each of its MTTKRP, inverse and solve launches records the first CTA entry
+ * and the last CTA exit (%globaltimer, ns). tsr_ctx_read_trace copies up to
+ * `capacity` records of the last call: start/end ns, kind (0 MTTKRP,
+ * 1 inverse, 2 solve) and mode, and the number written into *count. */
+int tsr_ctx_set_trace(tsr_ctx* ctx, int capacity);
+int tsr_ctx_read_trace(tsr_ctx* ctx, int capacity, int64_t* start_ns, int64_t* end_ns,
+                       int* kind, int* mode, int* count);
 
 /* ---- Khatri-Rao: crates/tenrso-kernels/src/khatri_rao.rs:56-89 ----------
  * out (I*J x K) with row a*J + b = A[a,:] * B[b,:]. Host pointers. */

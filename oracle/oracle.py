@@ -259,6 +259,52 @@ def coo_mttkrp(idx, vals, shape, factors, mode):
     return out
 
 
+def cp_als_coo(idx, vals, shape, rank: int, max_iters: int, tol: float, init_factors):
+    """CP-ALS of a sparse tensor given as COO, in FP64: the loop of
+    ``cp_als`` (cp/core.rs:59-182; mode order, solve_least_squares restated
+    as the oracle's FP64 solve, fit of helpers.rs:513-530, stopping rules)
+    with every MTTKRP the FP64 sparse definition (coo_mttkrp) instead of the
+    dense unfolding. tenrso has no sparse cp_als: this is its dense loop on
+    the nonzeros, for tensors too large to densify. Returns (factors, info)."""
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    U = [np.array(f, dtype=np.float64) for f in init_factors]
+    N = len(shape)
+    xn = float(vals @ vals)
+    prev_fit, fit, osc, change, reason = 0.0, 0.0, 0, 0.0, "MaxIterations"
+    hist, iters = [], 0
+    for it in range(max_iters):
+        iters = it + 1
+        M = None
+        for n in range(N):
+            M = coo_mttkrp(idx, vals, shape, U, n)
+            G = np.ones((rank, rank))
+            for m in range(N):
+                if m != n:
+                    G *= gram(U[m])
+            U[n] = solve(M, G)
+        # <X, Xhat> from the last mode's MTTKRP (equal to compute_inner_product)
+        inner = float(np.sum(M * U[N - 1]))
+        H = np.ones((rank, rank))
+        for f in U:
+            H *= gram(f)
+        err = np.sqrt(max(xn + float(H.sum()) - 2.0 * inner, 0.0))
+        fit = min(max(1.0 - err / np.sqrt(xn), 0.0), 1.0)
+        hist.append(fit)
+        if it > 0 and fit < prev_fit:
+            osc += 1
+        change = abs(fit - prev_fit)
+        if it > 0 and change < tol:
+            reason = "FitTolerance"
+            break
+        if osc > 5 and it > 10:
+            reason = "Oscillation"
+            break
+        prev_fit = fit
+    info = dict(fit=fit, iters=iters, reason=reason, oscillation_count=osc, oscillated=osc > 0,
+                final_fit_change=change, fit_history=np.asarray(hist))
+    return U, info
+
+
 def cp_reconstruct(factors, weights=None):
     """Restated ``tenrso_kernels::cp_reconstruct`` (outer.rs:223-274), FP64."""
     fs = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]

@@ -51,6 +51,8 @@ SIGNATURES = {
     "tsr_ctx_synchronize": (C.c_int, [P]),
     "tsr_ctx_launch_count": (I64, [P]),
     "tsr_ctx_set_wait_budget": (C.c_int, [P, I64]),
+    "tsr_ctx_set_trace": (C.c_int, [P, C.c_int]),
+    "tsr_ctx_read_trace": (C.c_int, [P, C.c_int, P, P, P, P, C.POINTER(C.c_int)]),
     "tsr_khatri_rao_f32": (C.c_int, [P, P, I64, I64, P, I64, I64, P]),
     "tsr_mttkrp_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, P]),
     "tsr_mttkrp_blocked_f32": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P, P, C.c_int, I64,

@@ -111,28 +111,31 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
 // so U follows from the pivot rows with the sign of the processed entries
 // flipped: a step needs the two pivot rows only.
 //
-// Roles (kGjThreads = 288 threads):
-//   bulk warps 0..7   thread (ty, tx) of a 16 x 16 grid owns rows ty + 16a and
-//                     columns tx + 16b (RB x RB doubles in registers) and only
-//                     applies the published updates: per step 2 RB 16-byte
-//                     shared loads and 2 RB^2 FMAs. During step s the owners
-//                     of rows 2s+4 and 2s+5 also copy them, updated through
-//                     step s, into a staging buffer.
-//   pivot warp 8      the serial chain: at step s it takes rows 2s+2, 2s+3
-//                     (staged during step s-1), applies step s to them, forms
-//                     U and W of step s+1 and publishes them. It holds no
-//                     other row, so its chain is not queued behind the bulk
-//                     FMAs; one barrier per step.
-// A pivot that is not positive, not finite or below 1e-290 (a non-positive
-// diagonal included) sets the "not SPD" flag, read once after the last step.
-constexpr int kGjThreads = 288;
+// Roles (kGjThreads = 544 threads; N = 16 RB, row blocks of 32):
+//   bulk warps 0..15  thread (ty, tx) of a 32 x 16 grid owns rows ty + 32a
+//                     (a < RA) and columns tx + 16b (b < RB) in registers and
+//                     only applies the published updates: per step RA + RB
+//                     16-byte shared loads and 2 RA RB FMAs. During step s the
+//                     owners of rows 2s+4 and 2s+5 (one warp) also copy them,
+//                     updated through step s, into a staging buffer.
+//   pivot warp 16     the serial chain. Lane l holds both rows of the next
+//                     pivot pair at columns l + 32c: at step s it takes rows
+//                     2s+2, 2s+3 as staged during step s-1, applies step s,
+//                     reads the 2 x 2 block with three shuffles, and writes U
+//                     and W of step s+1 for its own columns.
+// One barrier per step. A pivot that is not positive, not finite or below
+// 1e-290 (a non-positive diagonal included) sets the "not SPD" flag, read once
+// after the last step.
+constexpr int kGjBulk = 512;
+constexpr int kGjThreads = kGjBulk + 32;
 
 template <int RB>
 struct GjShared {
-  double2 u[2][16 * RB];        // [buffer][row]: (U[i][0], U[i][1]) of the step
-  double2 w[2][16 * RB];        // [buffer][column]: (W[j][0], W[j][1]) of the step
-  double stage[2][2][16 * RB];  // [slot][pivot row of the pair][column]
-  double dsc[16 * RB];          // the diagonal scaling 1 / sqrt(G_ii)
+  static constexpr int NP = 32 * ((RB + 1) / 2);  // rows padded to whole 32-row blocks
+  double2 u[2][NP];        // [buffer][row]: (U[i][0], U[i][1]) of the step
+  double2 w[2][NP];        // [buffer][column]: (W[j][0], W[j][1]) of the step
+  double stage[2][2][NP];  // [slot][pivot row of the pair][column]
+  double dsc[NP];          // the diagonal scaling 1 / sqrt(G_ii)
   double scale;
   int bad;
 };
@@ -148,25 +151,26 @@ __device__ __forceinline__ double recip_nr(double p) {
   return x;
 }
 
-// Called by the pivot warp holding rows k and k+1 (k even): lanes 0-15 hold
-// row k, lanes 16-31 row k+1, at columns tx + 16 bj (`row`, their values after
-// every earlier step). Publishes U and W of the step into buffer `buf`.
+// The pivot warp: r0/r1 hold rows k and k+1 (k even, their values after every
+// earlier step) at columns lane + 32c. Publishes U and W of the step into
+// buffer `buf` for those columns.
 template <int RB>
-__device__ __forceinline__ void gj2_publish(const double (&row)[RB], int k, int buf,
+__device__ __forceinline__ void gj2_publish(const double (&r0)[(RB + 1) / 2],
+                                            const double (&r1)[(RB + 1) / 2], int k, int buf,
                                             GjShared<RB>& sh) {
-  const int lane = threadIdx.x & 31, tx = lane & 15, half = lane >> 4;
-  const int kb = k >> 4, kt = k & 15;  // columns k and k+1 are kt, kt+1 of block kb
-  // the partner row's values at this lane's columns (independent of the pivot)
-  double o[RB];
+  constexpr int N = 16 * RB, CP = (RB + 1) / 2;
+  const int lane = threadIdx.x & 31;
+  const int ck = k >> 5, lk = k & 31;  // columns k, k+1: lanes lk, lk+1 of block ck
+  double m0 = r0[0], m1 = r1[0];
 #pragma unroll
-  for (int bj = 0; bj < RB; ++bj) o[bj] = __shfl_xor_sync(0xffffffffu, row[bj], 16);
-  double mine = row[0];
-#pragma unroll
-  for (int bj = 1; bj < RB; ++bj)
-    if (bj == kb) mine = row[bj];
-  const double a = __shfl_sync(0xffffffffu, mine, kt);           // A[k][k]
-  const double b = __shfl_sync(0xffffffffu, mine, kt + 1);       // A[k][k+1]
-  const double d = __shfl_sync(0xffffffffu, mine, 16 + kt + 1);  // A[k+1][k+1]
+  for (int c = 1; c < CP; ++c)
+    if (c == ck) {
+      m0 = r0[c];
+      m1 = r1[c];
+    }
+  const double a = __shfl_sync(0xffffffffu, m0, lk);      // A[k][k]
+  const double b = __shfl_sync(0xffffffffu, m0, lk + 1);  // A[k][k+1]
+  const double d = __shfl_sync(0xffffffffu, m1, lk + 1);  // A[k+1][k+1]
   const double det = fma(a, d, -(b * b));
   // LDL^T pivots a and det / a
   const bool good = a >= 1e-290 && det >= 1e-290 * a && isfinite(a) && isfinite(det);
@@ -174,26 +178,22 @@ __device__ __forceinline__ void gj2_publish(const double (&row)[RB], int k, int 
   const double id = recip_nr(good ? det : 1.0);
   const double p00 = d * id, p01 = -b * id, p11 = a * id;  // P^-1 (symmetric)
 #pragma unroll
-  for (int bj = 0; bj < RB; ++bj) {
-    const int j = tx + 16 * bj;
-    const double r = row[bj];
-    const double r0 = half ? o[bj] : r, r1 = half ? r : o[bj];
-    double w0 = fma(p00, r0, p01 * r1), w1 = fma(p01, r0, p11 * r1);
-    const double sg = j < k ? -1.0 : 1.0;
-    double u0 = sg * r0, u1 = sg * r1;
-    if (j == k) {
-      w0 = 1.0 + p00;
-      w1 = p01;
-      u0 = a - 1.0;
-      u1 = b;
-    } else if (j == k + 1) {
-      w0 = p01;
-      w1 = 1.0 + p11;
-      u0 = b;
-      u1 = d - 1.0;
-    }
-    // the two half-warps hold the same columns: one writes each pair
-    if (half == 0) {
+  for (int c = 0; c < CP; ++c) {
+    const int j = lane + 32 * c;
+    if (j < N) {
+      double w0 = fma(p00, r0[c], p01 * r1[c]), w1 = fma(p01, r0[c], p11 * r1[c]);
+      double u0 = j < k ? -r0[c] : r0[c], u1 = j < k ? -r1[c] : r1[c];
+      if (j == k) {
+        w0 = 1.0 + p00;
+        w1 = p01;
+        u0 = a - 1.0;
+        u1 = b;
+      } else if (j == k + 1) {
+        w0 = p01;
+        w1 = 1.0 + p11;
+        u0 = b;
+        u1 = d - 1.0;
+      }
       sh.w[buf][j] = make_double2(w0, w1);
       sh.u[buf][j] = make_double2(u0, u1);
     }
@@ -202,91 +202,100 @@ __device__ __forceinline__ void gj2_publish(const double (&row)[RB], int k, int 
 
 // Whole CTA (kGjThreads). `a` is meaningful in the bulk threads only.
 template <int RB>
-__device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
-  constexpr int N = 16 * RB;
+__device__ bool gj_inverse(double (&a)[(RB + 1) / 2][RB], GjShared<RB>& sh) {
+  constexpr int N = 16 * RB, RA = (RB + 1) / 2;
   constexpr int STEPS = N / 2;
-  const bool bulk = threadIdx.x < 256;
-  const int tx = threadIdx.x & 15, ty = (threadIdx.x >> 4) & 15;
+  const bool bulk = threadIdx.x < kGjBulk;
+  const int tx = threadIdx.x & 15, ty = (threadIdx.x >> 4) & 31;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // diagonal scaling (a non-positive diagonal scales its row to zero, whose
   // pivot then reports "not SPD")
   if (threadIdx.x == 0) sh.bad = 0;
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj)
-        if (ty + 16 * ai == tx + 16 * bj) {
+        if (ty + 32 * ai == tx + 16 * bj) {
           const double g = a[ai][bj];
-          sh.dsc[ty + 16 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
+          sh.dsc[ty + 32 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
         }
   }
   __syncthreads();
-  double di[RB], dj[RB];
+  double di[RA], dj[RB];
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai) di[ai] = sh.dsc[ty + 16 * ai];
+  for (int ai = 0; ai < RA; ++ai) di[ai] = ty + 32 * ai < N ? sh.dsc[ty + 32 * ai] : 0.0;
 #pragma unroll
   for (int bj = 0; bj < RB; ++bj) dj[bj] = sh.dsc[tx + 16 * bj];
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
-    // rows 0, 1 (step 0's pivots) into slot 0 and rows 2, 3 into slot 1
+    // rows 0, 1 (step 0's pivots) into slot 0 and rows 2, 3 into slot 1:
+    // warp 0 owns rows 0 and 1 (ty 0, 1), warp 1 rows 2 and 3
     if (warp <= 1) {
-      const int h = ty & 1;
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) sh.stage[warp][h][tx + 16 * bj] = a[0][bj];
+      for (int bj = 0; bj < RB; ++bj) sh.stage[warp][ty & 1][tx + 16 * bj] = a[0][bj];
     }
   }
   __syncthreads();
-  double prow[RB];  // pivot warp: its two rows (lanes 0-15 first, 16-31 second)
+  constexpr int CP = RA;
+  double r0[CP], r1[CP];  // pivot warp: the pair's two rows at columns lane + 32c
   if (!bulk) {
-    const int h = lane >> 4;
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) prow[bj] = sh.stage[0][h][tx + 16 * bj];
-    gj2_publish<RB>(prow, 0, 0, sh);
+    for (int c = 0; c < CP; ++c) {
+      const int j = lane + 32 * c;
+      r0[c] = j < N ? sh.stage[0][0][j] : 0.0;
+      r1[c] = j < N ? sh.stage[0][1][j] : 0.0;
+    }
+    gj2_publish<RB>(r0, r1, 0, 0, sh);
   }
   __syncthreads();
 #pragma unroll 1
   for (int s = 0; s < STEPS; ++s) {
     const int buf = s & 1, k = 2 * s;
     if (bulk) {
-      double2 u[RB], w[RB];
+      double2 u[RA], w[RB];
 #pragma unroll
-      for (int ai = 0; ai < RB; ++ai) u[ai] = sh.u[buf][ty + 16 * ai];
+      for (int ai = 0; ai < RA; ++ai)
+        u[ai] = ty + 32 * ai < N ? sh.u[buf][ty + 32 * ai] : make_double2(0.0, 0.0);
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) w[bj] = sh.w[buf][tx + 16 * bj];
 #pragma unroll
-      for (int ai = 0; ai < RB; ++ai)
+      for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
         for (int bj = 0; bj < RB; ++bj)
           a[ai][bj] = fma(-u[ai].x, w[bj].x, fma(-u[ai].y, w[bj].y, a[ai][bj]));
       // rows k+4, k+5 (step s+2's pivots), updated through step s, to the
-      // pivot warp: staged in slot s & 1
+      // pivot warp: staged in slot s & 1 (one warp owns both rows)
       const int k4 = k + 4;
-      if (k4 < N && warp == ((k4 & 15) >> 1)) {
-        const int kb4 = k4 >> 4, h = ty & 1;
+      if (k4 < N && warp == ((k4 & 31) >> 1)) {
+        const int ab = k4 >> 5;
 #pragma unroll
         for (int bj = 0; bj < RB; ++bj) {
           double v = a[0][bj];
 #pragma unroll
-          for (int ai = 1; ai < RB; ++ai)
-            if (ai == kb4) v = a[ai][bj];
-          sh.stage[buf][h][tx + 16 * bj] = v;
+          for (int ai = 1; ai < RA; ++ai)
+            if (ai == ab) v = a[ai][bj];
+          sh.stage[buf][ty & 1][tx + 16 * bj] = v;
         }
       }
     } else if (s + 1 < STEPS) {
-      // rows k+2, k+3 as of step s-1 (staged during step s-1, slot (s+1) & 1),
-      // step s applied, then step s+1 published
-      const int h = lane >> 4, k2 = k + 2;
-      const double2 ur = sh.u[buf][k2 + h];
+      // rows k+2, k+3 as staged during step s-1 (slot (s+1) & 1), step s
+      // applied, then step s+1 published
+      const int k2 = k + 2;
+      const double2 ua = sh.u[buf][k2], ub = sh.u[buf][k2 + 1];
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) {
-        const double2 wv = sh.w[buf][tx + 16 * bj];
-        prow[bj] = fma(-ur.x, wv.x, fma(-ur.y, wv.y, sh.stage[buf ^ 1][h][tx + 16 * bj]));
+      for (int c = 0; c < CP; ++c) {
+        const int j = lane + 32 * c;
+        if (j < N) {
+          const double2 wv = sh.w[buf][j];
+          r0[c] = fma(-ua.x, wv.x, fma(-ua.y, wv.y, sh.stage[buf ^ 1][0][j]));
+          r1[c] = fma(-ub.x, wv.x, fma(-ub.y, wv.y, sh.stage[buf ^ 1][1][j]));
+        }
       }
-      gj2_publish<RB>(prow, k2, buf ^ 1, sh);
+      gj2_publish<RB>(r0, r1, k2, buf ^ 1, sh);
     }
     __syncthreads();
   }
@@ -294,46 +303,48 @@ __device__ bool gj_inverse(double (&a)[RB][RB], GjShared<RB>& sh) {
   // G^-1 = D G'^-1 D
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
   }
   return true;
 }
 
-// G(i, j) = prod_{m != mode} Gram_m(i, j) for this thread's RB x RB block. All
-// loads are issued before any store (grams and hadam are distinct buffers).
+// G(i, j) = prod_{m != mode} Gram_m(i, j) for this bulk thread's entries
+// (rows ty + 32a, columns tx + 16b). All loads are issued before any store
+// (grams and hadam are distinct buffers).
 template <int RB>
 __device__ void load_hadamard(const double* __restrict__ grams, double* __restrict__ hadam,
-                              int ndim, int mode, int R, double ridge, double (&a)[RB][RB],
-                              bool write_h) {
+                              int ndim, int mode, int R, double ridge,
+                              double (&a)[(RB + 1) / 2][RB], bool write_h) {
+  constexpr int RA = (RB + 1) / 2;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int RR = R * R;
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+  for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
     for (int bj = 0; bj < RB; ++bj) a[ai][bj] = 1.0;  // helpers.rs:414 starts from ones
   for (int m = 0; m < ndim; ++m) {
     if (m == mode) continue;
     const double* g = grams + (int64_t)m * RR;
-    double v[RB][RB];
+    double v[RA][RB];
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) {
-        const int i = ty + 16 * ai, j = tx + 16 * bj;
+        const int i = ty + 32 * ai, j = tx + 16 * bj;
         v[ai][bj] = (i < R && j < R) ? __ldg(g + (i <= j ? i * R + j : j * R + i)) : 1.0;
       }
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= v[ai][bj];
   }
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+  for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
     for (int bj = 0; bj < RB; ++bj) {
-      const int i = ty + 16 * ai, j = tx + 16 * bj;
+      const int i = ty + 32 * ai, j = tx + 16 * bj;
       if (i < R && j < R) {
         if (write_h) hadam[(int64_t)mode * RR + i * R + j] = a[ai][bj];
         if (i == j) a[ai][bj] += ridge;
@@ -343,15 +354,16 @@ __device__ void load_hadamard(const double* __restrict__ grams, double* __restri
     }
 }
 
-// a += l2 * I on this thread's RB x RB block (the ridge of cp_als_constrained)
+// a += l2 * I on this bulk thread's entries (the ridge of cp_als_constrained)
 template <int RB>
-__device__ __forceinline__ void add_diagonal(double (&a)[RB][RB], int R, double l2) {
+__device__ __forceinline__ void add_diagonal(double (&a)[(RB + 1) / 2][RB], int R, double l2) {
+  constexpr int RA = (RB + 1) / 2;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
+  for (int ai = 0; ai < RA; ++ai)
 #pragma unroll
     for (int bj = 0; bj < RB; ++bj)
-      if (ty + 16 * ai == tx + 16 * bj && ty + 16 * ai < R) a[ai][bj] += l2;
+      if (ty + 32 * ai == tx + 16 * bj && ty + 32 * ai < R) a[ai][bj] += l2;
 }
 
 // fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
@@ -417,10 +429,11 @@ __global__ void fit_kernel(AlsBuffers b, double tol) {
 // solve_least_squares does, helpers.rs:477-490); zeroes this mode's Gram
 // accumulator (and <X,Xhat> for the last mode) for the solve that follows.
 template <int RB>
-__global__ void __launch_bounds__(kGjThreads) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
+__global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
                                                    float ridge_eps, int last, double tol,
-                                                   double l2) {
+                                                   double l2, TraceSlot tr) {
   __shared__ GjShared<RB> gsh;
+  trace_begin(tr);
   AlsState* st = b.state;
   if (st->done) return;
   if (mode == 0 && st->fit_pending) {
@@ -430,10 +443,10 @@ __global__ void __launch_bounds__(kGjThreads) chol_kernel(AlsBuffers b, int ndim
     if (*(volatile int*)&st->done) return;
   }
   const int RR = R * R;
-  // threads 0..255 hold the matrix, 16 x 16 grid (RB x RB each); warp 8 is
-  // the inverse's pivot warp
-  const bool bulk = threadIdx.x < 256;
-  double a[RB][RB];
+  // threads 0..511 hold the matrix, 32 x 16 grid; warp 16 is the inverse's
+  // pivot warp
+  const bool bulk = threadIdx.x < kGjBulk;
+  double a[(RB + 1) / 2][RB];
   if (bulk) {
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
     if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
@@ -483,10 +496,10 @@ __global__ void __launch_bounds__(kGjThreads) chol_kernel(AlsBuffers b, int ndim
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RB; ++ai)
+    for (int ai = 0; ai < (RB + 1) / 2; ++ai)
 #pragma unroll
       for (int bj = 0; bj < RB; ++bj) {
-        const int i = ty + 16 * ai, j = tx + 16 * bj;
+        const int i = ty + 32 * ai, j = tx + 16 * bj;
         if (i < R && j < R) b.ginv[i * R + j] = a[ai][bj];
       }
   }
@@ -496,6 +509,7 @@ __global__ void __launch_bounds__(kGjThreads) chol_kernel(AlsBuffers b, int ndim
     st->inner = 0.0;
     st->xhat_sq = 0.0;
   }
+  trace_end(tr);
 }
 
 // Thread groups per element in the split sums of a chunk of `full` outputs:
@@ -528,10 +542,12 @@ template <int RB>
 __global__ void __launch_bounds__(256)
 solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64_t rows, int R,
              int rpc, float* __restrict__ U, double* __restrict__ gram, int last, int ndim,
-             double tol, float l1, int nonneg, uint8_t* __restrict__ bimg, int img_n_pad) {
+             double tol, float l1, int nonneg, uint8_t* __restrict__ bimg, int img_n_pad,
+             TraceSlot tr) {
   extern __shared__ __align__(16) double sh[];
   __shared__ __align__(8) uint64_t gi_bar;
   __shared__ int gi_state;  // 0 copy in flight, 1 landed, 2 gave up
+  trace_begin(tr);
   if (threadIdx.x == 0) grid_dep_trigger();
   AlsState* st = b.state;
   if (st->done) return;
@@ -715,7 +731,10 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
       const int a = ty + 16 * ai, c = tx + 16 * bj;
       if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
     }
-  if (!last) return;
+  if (!last) {
+    trace_end(tr);
+    return;
+  }
   // ||Xhat||^2 = sum_ac H_ac (U^T U)_ac with H the Hadamard of the other
   // Grams (this mode's inverse kernel wrote it): this CTA's share from its
   // Gram blocks, off-diagonal entries counted twice
@@ -751,6 +770,7 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
   // the fit of this sweep is formed by the next inverse kernel (or by
   // fit_kernel after the last sweep), once this grid's atomics are complete
   if (blockIdx.x == 0 && threadIdx.x == 0) st->fit_pending = 1;
+  trace_end(tr);
 }
 
 }  // namespace
@@ -798,15 +818,16 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
                 float ridge_eps, bool last, double tol, double l2) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
+  const TraceSlot tr = trace_slot(ctx, TRACE_INVERSE, mode);
   const int lst = last ? 1 : 0;
   switch ((R + 15) / 16) {
-    case 1: chol_kernel<1><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 2: chol_kernel<2><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 3: chol_kernel<3><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 4: chol_kernel<4><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 5: chol_kernel<5><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    case 6: chol_kernel<6><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
-    default: chol_kernel<7><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2); break;
+    case 1: chol_kernel<1><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    case 2: chol_kernel<2><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    case 3: chol_kernel<3><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    case 4: chol_kernel<4><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    case 5: chol_kernel<5><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    case 6: chol_kernel<6><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+    default: chol_kernel<7><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
   }
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
@@ -853,9 +874,11 @@ int launch_solve(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, const float*
   const size_t smem = (size_t)(R * R + 2 * full + (size_t)groups * full) * sizeof(double);
   if (smem > 200 * 1024) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const int lst = last ? 1 : 0;
+  // the mode is the Gram slot this solve accumulates into
+  const TraceSlot tr = trace_slot(ctx, TRACE_SOLVE, (int)((gram - b.grams) / ((int64_t)R * R)));
 #define TSR_SOLVE(RB)                                                                    \
   TSR_CUDA(launch_pdl(solve_kernel<RB>, dim3(grid), dim3(256), smem, s, b, partials, splits, \
-                      rows, R, rpc, U, gram, lst, ndim, tol, l1, nonneg, bimg, img_n_pad))
+                      rows, R, rpc, U, gram, lst, ndim, tol, l1, nonneg, bimg, img_n_pad, tr))
   switch ((R + 15) / 16) {
     case 1: TSR_SOLVE(1); break;
     case 2: TSR_SOLVE(2); break;

@@ -80,6 +80,28 @@ enum Slot {
 
 }  // namespace tsr
 
+namespace tsr {
+// Kernel timeline tracing of the CP-ALS sweep (off unless enabled on the
+// context): each traced launch owns one slot; every CTA's thread 0 folds the
+// %globaltimer value at entry into start (min) and at exit into end (max).
+struct TraceSlot {
+  unsigned long long* start;
+  unsigned long long* end;
+};
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void trace_begin(const TraceSlot& tr) {
+  if (tr.start && threadIdx.x == 0) atomicMin(tr.start, globaltimer_ns());
+}
+__device__ __forceinline__ void trace_end(const TraceSlot& tr) {
+  if (tr.end && threadIdx.x == 0) atomicMax(tr.end, globaltimer_ns());
+}
+enum TraceKind { TRACE_MTTKRP = 0, TRACE_INVERSE = 1, TRACE_SOLVE = 2 };
+}  // namespace tsr
+
 struct tsr_ctx {
   int device = 0;
   int sm_count = 148;
@@ -95,6 +117,13 @@ struct tsr_ctx {
   // MTTKRP (about 1 s by default; tsr_ctx_set_wait_budget lowers it to test
   // the timeout path)
   long long wait_budget = 1ll << 31;
+  // kernel timeline tracing (tsr_ctx_set_trace): device start/end arrays,
+  // the next free slot and, per slot, the kernel kind and mode
+  unsigned long long* trace_start = nullptr;
+  unsigned long long* trace_end = nullptr;
+  int trace_cap = 0;
+  int trace_next = 0;
+  std::vector<std::pair<int, int>> trace_meta;
   // SMs the MTTKRP grids leave free so that the side-stream FP64 kernels of
   // the ALS sweep (Gram, inverse, fit) run concurrently instead of queueing
   int reserve_sms = 8;
@@ -125,6 +154,9 @@ int read_status(tsr_ctx* ctx, unsigned* out);  // synchronizes the stream
 // Evict L2 by reading a buffer of twice its size (clean lines only).
 int flush_l2(tsr_ctx* ctx, cudaStream_t s);
 int reset_status(tsr_ctx* ctx);
+// The next trace slot for a launch of `kind` on `mode` ({nullptr, nullptr}
+// when tracing is off or the buffer is full).
+TraceSlot trace_slot(tsr_ctx* ctx, int kind, int mode);
 // Synchronizes, reads and clears the status word: TSR_E_TIMEOUT when a
 // kernel's bounded wait gave up, else TSR_OK.
 int check_device_status(tsr_ctx* ctx);

@@ -107,6 +107,17 @@ int reset_status(tsr_ctx* ctx) {
   return TSR_OK;
 }
 
+TraceSlot trace_slot(tsr_ctx* ctx, int kind, int mode) {
+  TraceSlot t{nullptr, nullptr};
+  if (!ctx->trace_start || ctx->trace_next >= ctx->trace_cap) return t;
+  const int i = ctx->trace_next++;
+  if ((int)ctx->trace_meta.size() <= i) ctx->trace_meta.resize(i + 1);
+  ctx->trace_meta[i] = {kind, mode};
+  t.start = ctx->trace_start + i;
+  t.end = ctx->trace_end + i;
+  return t;
+}
+
 int check_device_status(tsr_ctx* ctx) {
   unsigned st = 0;
   TSR_TRY(read_status(ctx, &st));
@@ -424,6 +435,7 @@ int tsr_ctx_destroy(tsr_ctx* ctx) {
     if (b.ptr) cudaFree(b.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->trace_start) cudaFree(ctx->trace_start);
   for (auto& g : ctx->sweep_graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& ev : ctx->ev)
@@ -441,6 +453,47 @@ int tsr_ctx_synchronize(tsr_ctx* ctx) {
 }
 
 int64_t tsr_ctx_launch_count(const tsr_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int tsr_ctx_set_trace(tsr_ctx* ctx, int capacity) {
+  TSR_TRY(check_ctx(ctx));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->trace_start) cudaFree(ctx->trace_start);
+  ctx->trace_start = ctx->trace_end = nullptr;
+  ctx->trace_cap = ctx->trace_next = 0;
+  ctx->trace_meta.clear();
+  for (auto& g : ctx->sweep_graphs)  // graphs captured with the old slots
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  ctx->sweep_graphs.clear();
+  if (capacity <= 0) return TSR_OK;
+  void* p = nullptr;
+  TSR_CUDA(cudaMalloc(&p, 2 * sizeof(unsigned long long) * (size_t)capacity));
+  ctx->trace_start = (unsigned long long*)p;
+  ctx->trace_end = ctx->trace_start + capacity;
+  ctx->trace_cap = capacity;
+  return TSR_OK;
+}
+
+int tsr_ctx_read_trace(tsr_ctx* ctx, int capacity, int64_t* start_ns, int64_t* end_ns,
+                       int* kind, int* mode, int* count) {
+  TSR_TRY(check_ctx(ctx));
+  if (!count) return fail(TSR_E_INVALID_ARG, "null count");
+  const int n = std::min(ctx->trace_next, capacity);
+  *count = n;
+  if (n <= 0 || !ctx->trace_start) return TSR_OK;
+  std::vector<unsigned long long> s(n), e(n);
+  TSR_CUDA(cudaMemcpyAsync(s.data(), ctx->trace_start, sizeof(unsigned long long) * n,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(e.data(), ctx->trace_end, sizeof(unsigned long long) * n,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; ++i) {
+    if (start_ns) start_ns[i] = (int64_t)s[i];
+    if (end_ns) end_ns[i] = (int64_t)e[i];
+    if (kind) kind[i] = ctx->trace_meta[i].first;
+    if (mode) mode[i] = ctx->trace_meta[i].second;
+  }
+  return TSR_OK;
+}
 
 int tsr_ctx_set_wait_budget(tsr_ctx* ctx, int64_t cycles) {
   TSR_TRY(check_ctx(ctx));

@@ -395,6 +395,14 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   TSR_CUDA(cudaMemsetAsync(stp, 0, sbytes, ctx->stream));
   TSR_CUDA(cudaMemsetAsync(gp, 0, gbytes, ctx->stream));
   TSR_TRY(reset_status(ctx));  // the MTTKRP kernels' status word
+  const bool tracing = ctx->trace_start != nullptr;
+  if (tracing) {  // this call's launches take slots from 0
+    ctx->trace_next = 0;
+    TSR_CUDA(cudaMemsetAsync(ctx->trace_start, 0xFF, sizeof(unsigned long long) * ctx->trace_cap,
+                             ctx->stream));
+    TSR_CUDA(cudaMemsetAsync(ctx->trace_end, 0, sizeof(unsigned long long) * ctx->trace_cap,
+                             ctx->stream));
+  }
   if (cons && cons->nonnegative && cons->validate_nonneg_input) {
     // helpers.rs:705-716: one pass over X before any factor is touched
     TSR_TRY(launch_any_negative(ctx, ctx->stream, dX, n, &a.b.state->pad));
@@ -530,8 +538,9 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     auto graph_for = [&](int nsweeps, tsr_ctx::SweepGraph** out) -> int {
       std::vector<uint8_t> key((const uint8_t*)&a, (const uint8_t*)&a + sizeof(a));
       key.insert(key.end(), (const uint8_t*)&nsweeps, (const uint8_t*)&nsweeps + sizeof(nsweeps));
+      // a traced call captures afresh, so its launches own this call's slots
       for (auto& g : ctx->sweep_graphs)
-        if (g.exec && g.key == key) {
+        if (g.exec && g.key == key && !tracing) {
           g.last_use = ++ctx->graph_clock;
           *out = &g;
           return TSR_OK;

@@ -73,6 +73,7 @@ struct M3Params {
   unsigned* status;
   long long wait_budget;  // clock cycles for each pipeline wait
   int a_resident;         // X's halves were written before the preceding kernel
+  TraceSlot tr;           // timeline tracing (null pointers when off)
 };
 
 __device__ __forceinline__ uint64_t evict_last_policy() {
@@ -139,6 +140,7 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
   const int nsteps = nruns * spr;
   const int acc_cols = 2 * p.n_pad;  // one accumulator: hh | cr
   const int tmem_cols = 2 * acc_cols;
+  trace_begin(p.tr);
   if (threadIdx.x == 0) grid_dep_trigger();
 
   if (threadIdx.x == 0) {
@@ -394,6 +396,7 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
     tc_fence_after();
     tmem_dealloc(tmem, (uint32_t)tmem_cols);
   }
+  trace_end(p.tr);
 }
 
 // X (fp32) -> bf16 hi = rn(x), lo = rn(x - hi), same layout; ||X||^2 in FP64
@@ -597,6 +600,7 @@ int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, cons
   q.status = ctx->d_status;
   q.wait_budget = ctx->wait_budget;
   q.a_resident = a_resident ? 1 : 0;
+  q.tr = trace_slot(ctx, TRACE_MTTKRP, mode);
   if (q.runs_per_split < 1 || q.runs_per_split > M3_MAX_RUNS)
     return fail(TSR_E_INVALID_ARG, "MTTKRP split plan out of range");
   int stages = 4;

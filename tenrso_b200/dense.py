@@ -39,6 +39,29 @@ class Context:
     def launches(self) -> int:
         return int(self._lib.tsr_ctx_launch_count(self.handle))
 
+    def set_trace(self, capacity: int = 4096):
+        """Turn kernel timeline tracing of dense cp_als calls on (capacity
+        slots) or off (0)."""
+        check(self._lib.tsr_ctx_set_trace(self.handle, int(capacity)))
+        self._trace_cap = int(capacity)
+
+    def read_trace(self):
+        """Records of the last traced cp_als call: a list of
+        (kind, mode, start_ns, end_ns), kind one of "mttkrp", "inverse",
+        "solve", in launch order."""
+        cap = getattr(self, "_trace_cap", 0)
+        if cap <= 0:
+            return []
+        st = np.zeros(cap, np.int64)
+        en = np.zeros(cap, np.int64)
+        kd = np.zeros(cap, np.int32)
+        md = np.zeros(cap, np.int32)
+        n = C.c_int(0)
+        check(self._lib.tsr_ctx_read_trace(self.handle, cap, _ptr(st), _ptr(en), _ptr(kd),
+                                           _ptr(md), C.byref(n)))
+        names = ("mttkrp", "inverse", "solve")
+        return [(names[kd[i]], int(md[i]), int(st[i]), int(en[i])) for i in range(n.value)]
+
     def set_wait_budget(self, cycles: int = 0):
         """Budget (clock cycles) of each bounded wait in the tensor-core MTTKRP;
         0 restores the default (about one second)."""

@@ -205,3 +205,18 @@ def test_oracle_reproduces_c2_fit_fixture(orc):
     assert np.max(np.abs(np.asarray(got["fp64_fit_history"]) -
                          np.asarray(ref["fp64_fit_history"]))) <= 1e-12
     assert abs(got["fp32_fit"] - ref["fp32_fit"]) <= 1e-6
+
+
+def test_cp_als_coo_matches_dense_oracle(orc):
+    """oracle.cp_als_coo (the FP64 checker of the sparse CP-ALS at sizes that
+    cannot be densified) reproduces the dense oracle's cp_als on a tensor
+    with half its entries structurally zero."""
+    from tenrso_b200 import synth
+    shape = (30, 20, 10)
+    X, _ = synth.dense_lowrank(shape, 4, seed=5, dist="uniform", noise=0.01)
+    X[X < np.quantile(X, 0.5)] = 0
+    nz = np.argwhere(X != 0)
+    init = synth.init_factors(shape, 4, 5)
+    _, a = orc.cp_als_coo(nz, X[tuple(nz.T)], shape, 4, 8, 0.0, init)
+    _, b = orc.cp_als(X.astype(np.float64), 4, 8, 0.0, [f.astype(np.float64) for f in init])
+    assert np.abs(a["fit_history"] - b["fit_history"]).max() <= 1e-12
