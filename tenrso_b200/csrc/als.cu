@@ -111,31 +111,49 @@ __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* o
 // so U follows from the pivot rows with the sign of the processed entries
 // flipped: a step needs the two pivot rows only.
 //
-// Roles (kGjThreads = 544 threads; N = 16 RB, row blocks of 32):
-//   bulk warps 0..15  thread (ty, tx) of a 32 x 16 grid owns rows ty + 32a
-//                     (a < RA) and columns tx + 16b (b < RB) in registers and
-//                     only applies the published updates: per step RA + RB
-//                     16-byte shared loads and 2 RA RB FMAs. During step s the
-//                     owners of rows 2s+4 and 2s+5 (one warp) also copy them,
-//                     updated through step s, into a staging buffer.
-//   pivot warp 16     the serial chain. Lane l holds both rows of the next
-//                     pivot pair at columns l + 32c: at step s it takes rows
-//                     2s+2, 2s+3 as staged during step s-1, applies step s,
-//                     reads the 2 x 2 block with three shuffles, and writes U
-//                     and W of step s+1 for its own columns.
+// Roles (kGjThreads = 512 threads = 16 warps; warp w runs on scheduler w % 4):
+//   pivot warp 0      the serial chain, alone on its scheduler so that its
+//                     dependent FP64 operations do not queue behind bulk FMAs.
+//                     Lane l holds both rows of the next pivot pair at columns
+//                     l + 32c. At step s it reads the 2 x 2 block of step s+1
+//                     (its three entries follow from seven broadcast shared
+//                     loads and two FMAs each, without waiting for the rows),
+//                     applies step s to rows 2s+2, 2s+3 as staged during step
+//                     s-1, and writes U and W of step s+1 for its columns.
+//   bulk warps        the 12 warps on schedulers 1-3 (w % 4 != 0), a 16 x 24
+//                     grid: thread (ty, tx) owns rows ty + 16a (a < RB) and
+//                     columns tx + 24b (b < CB) in registers and only applies
+//                     the published updates. During step s the owners of rows
+//                     2s+4 and 2s+5 also copy them, updated through step s,
+//                     into a staging buffer.
+//   warps 4, 8, 12    idle (they keep scheduler 0 to the pivot warp).
 // One barrier per step. A pivot that is not positive, not finite or below
 // 1e-290 (a non-positive diagonal included) sets the "not SPD" flag, read once
 // after the last step.
-constexpr int kGjBulk = 512;
-constexpr int kGjThreads = kGjBulk + 32;
+constexpr int kGjThreads = 512;
+constexpr int kGjCW = 24;  // bulk grid width (columns per sweep of a thread)
+
+template <int RB>
+struct GjLayout {
+  static constexpr int N = 16 * RB;                   // padded matrix size
+  static constexpr int CB = (N + kGjCW - 1) / kGjCW;  // column blocks per bulk thread
+  static constexpr int CP = (N + 31) / 32;            // pivot-warp columns per lane
+};
+
+__device__ __forceinline__ bool gj_bulk() { return ((threadIdx.x >> 5) & 3) != 0; }
+// bulk thread index 0..383 (warps 1, 2, 3, 5, 6, 7, ... in order)
+__device__ __forceinline__ int gj_bulk_index() {
+  const int w = threadIdx.x >> 5;
+  return gj_bulk() ? (w - (w >> 2) - 1) * 32 + (threadIdx.x & 31) : 0;
+}
 
 template <int RB>
 struct GjShared {
-  static constexpr int NP = 32 * ((RB + 1) / 2);  // rows padded to whole 32-row blocks
-  double2 u[2][NP];        // [buffer][row]: (U[i][0], U[i][1]) of the step
-  double2 w[2][NP];        // [buffer][column]: (W[j][0], W[j][1]) of the step
-  double stage[2][2][NP];  // [slot][pivot row of the pair][column]
-  double dsc[NP];          // the diagonal scaling 1 / sqrt(G_ii)
+  static constexpr int N = 16 * RB;
+  double2 u[2][N];        // [buffer][row]: (U[i][0], U[i][1]) of the step
+  double2 w[2][N];        // [buffer][column]: (W[j][0], W[j][1]) of the step
+  double stage[2][2][N];  // [slot][pivot row of the pair][column]
+  double dsc[N];          // the diagonal scaling 1 / sqrt(G_ii)
   double scale;
   int bad;
 };
@@ -152,25 +170,15 @@ __device__ __forceinline__ double recip_nr(double p) {
 }
 
 // The pivot warp: r0/r1 hold rows k and k+1 (k even, their values after every
-// earlier step) at columns lane + 32c. Publishes U and W of the step into
-// buffer `buf` for those columns.
+// earlier step) at columns lane + 32c, and (a, b, d) = (A[k][k], A[k][k+1],
+// A[k+1][k+1]). Publishes U and W of the step into buffer `buf`.
 template <int RB>
-__device__ __forceinline__ void gj2_publish(const double (&r0)[(RB + 1) / 2],
-                                            const double (&r1)[(RB + 1) / 2], int k, int buf,
+__device__ __forceinline__ void gj2_publish(const double (&r0)[GjLayout<RB>::CP],
+                                            const double (&r1)[GjLayout<RB>::CP], double a,
+                                            double b, double d, int k, int buf,
                                             GjShared<RB>& sh) {
-  constexpr int N = 16 * RB, CP = (RB + 1) / 2;
+  constexpr int N = GjLayout<RB>::N, CP = GjLayout<RB>::CP;
   const int lane = threadIdx.x & 31;
-  const int ck = k >> 5, lk = k & 31;  // columns k, k+1: lanes lk, lk+1 of block ck
-  double m0 = r0[0], m1 = r1[0];
-#pragma unroll
-  for (int c = 1; c < CP; ++c)
-    if (c == ck) {
-      m0 = r0[c];
-      m1 = r1[c];
-    }
-  const double a = __shfl_sync(0xffffffffu, m0, lk);      // A[k][k]
-  const double b = __shfl_sync(0xffffffffu, m0, lk + 1);  // A[k][k+1]
-  const double d = __shfl_sync(0xffffffffu, m1, lk + 1);  // A[k+1][k+1]
   const double det = fma(a, d, -(b * b));
   // LDL^T pivots a and det / a
   const bool good = a >= 1e-290 && det >= 1e-290 * a && isfinite(a) && isfinite(det);
@@ -202,100 +210,106 @@ __device__ __forceinline__ void gj2_publish(const double (&r0)[(RB + 1) / 2],
 
 // Whole CTA (kGjThreads). `a` is meaningful in the bulk threads only.
 template <int RB>
-__device__ bool gj_inverse(double (&a)[(RB + 1) / 2][RB], GjShared<RB>& sh) {
-  constexpr int N = 16 * RB, RA = (RB + 1) / 2;
+__device__ bool gj_inverse(double (&a)[RB][GjLayout<RB>::CB], GjShared<RB>& sh) {
+  constexpr int N = GjLayout<RB>::N, CB = GjLayout<RB>::CB, CP = GjLayout<RB>::CP;
   constexpr int STEPS = N / 2;
-  const bool bulk = threadIdx.x < kGjBulk;
-  const int tx = threadIdx.x & 15, ty = (threadIdx.x >> 4) & 31;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool bulk = gj_bulk(), pivot = threadIdx.x < 32;
+  const int t = gj_bulk_index(), ty = t / kGjCW, tx = t % kGjCW;
+  const int lane = threadIdx.x & 31;
   // diagonal scaling (a non-positive diagonal scales its row to zero, whose
   // pivot then reports "not SPD")
   if (threadIdx.x == 0) sh.bad = 0;
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RA; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj)
-        if (ty + 32 * ai == tx + 16 * bj) {
+      for (int bj = 0; bj < CB; ++bj)
+        if (ty + 16 * ai == tx + kGjCW * bj) {
           const double g = a[ai][bj];
-          sh.dsc[ty + 32 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
+          sh.dsc[ty + 16 * ai] = (g > 0.0 && isfinite(g)) ? rsqrt(g) : 0.0;
         }
   }
   __syncthreads();
-  double di[RA], dj[RB];
+  double di[RB], dj[CB];
 #pragma unroll
-  for (int ai = 0; ai < RA; ++ai) di[ai] = ty + 32 * ai < N ? sh.dsc[ty + 32 * ai] : 0.0;
+  for (int ai = 0; ai < RB; ++ai) di[ai] = sh.dsc[ty + 16 * ai];
 #pragma unroll
-  for (int bj = 0; bj < RB; ++bj) dj[bj] = sh.dsc[tx + 16 * bj];
+  for (int bj = 0; bj < CB; ++bj) dj[bj] = tx + kGjCW * bj < N ? sh.dsc[tx + kGjCW * bj] : 0.0;
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RA; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
-    // rows 0, 1 (step 0's pivots) into slot 0 and rows 2, 3 into slot 1:
-    // warp 0 owns rows 0 and 1 (ty 0, 1), warp 1 rows 2 and 3
-    if (warp <= 1) {
+      for (int bj = 0; bj < CB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
+    // rows 0, 1 (step 0's pivots) into slot 0 and rows 2, 3 into slot 1
+    if (ty < 4) {
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) sh.stage[warp][ty & 1][tx + 16 * bj] = a[0][bj];
+      for (int bj = 0; bj < CB; ++bj)
+        if (tx + kGjCW * bj < N) sh.stage[ty >> 1][ty & 1][tx + kGjCW * bj] = a[0][bj];
     }
   }
   __syncthreads();
-  constexpr int CP = RA;
   double r0[CP], r1[CP];  // pivot warp: the pair's two rows at columns lane + 32c
-  if (!bulk) {
+  if (pivot) {
 #pragma unroll
     for (int c = 0; c < CP; ++c) {
       const int j = lane + 32 * c;
       r0[c] = j < N ? sh.stage[0][0][j] : 0.0;
       r1[c] = j < N ? sh.stage[0][1][j] : 0.0;
     }
-    gj2_publish<RB>(r0, r1, 0, 0, sh);
+    gj2_publish<RB>(r0, r1, sh.stage[0][0][0], sh.stage[0][0][1], sh.stage[0][1][1], 0, 0, sh);
   }
   __syncthreads();
 #pragma unroll 1
   for (int s = 0; s < STEPS; ++s) {
     const int buf = s & 1, k = 2 * s;
     if (bulk) {
-      double2 u[RA], w[RB];
+      double2 u[RB], w[CB];
 #pragma unroll
-      for (int ai = 0; ai < RA; ++ai)
-        u[ai] = ty + 32 * ai < N ? sh.u[buf][ty + 32 * ai] : make_double2(0.0, 0.0);
+      for (int ai = 0; ai < RB; ++ai) u[ai] = sh.u[buf][ty + 16 * ai];
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) w[bj] = sh.w[buf][tx + 16 * bj];
+      for (int bj = 0; bj < CB; ++bj)
+        w[bj] = tx + kGjCW * bj < N ? sh.w[buf][tx + kGjCW * bj] : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int ai = 0; ai < RA; ++ai)
+      for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-        for (int bj = 0; bj < RB; ++bj)
+        for (int bj = 0; bj < CB; ++bj)
           a[ai][bj] = fma(-u[ai].x, w[bj].x, fma(-u[ai].y, w[bj].y, a[ai][bj]));
       // rows k+4, k+5 (step s+2's pivots), updated through step s, to the
-      // pivot warp: staged in slot s & 1 (one warp owns both rows)
+      // pivot warp: staged in slot s & 1
       const int k4 = k + 4;
-      if (k4 < N && warp == ((k4 & 31) >> 1)) {
-        const int ab = k4 >> 5;
+      if (k4 < N && (ty >> 1) == ((k4 & 15) >> 1)) {
+        const int ab = k4 >> 4;
 #pragma unroll
-        for (int bj = 0; bj < RB; ++bj) {
+        for (int bj = 0; bj < CB; ++bj) {
           double v = a[0][bj];
 #pragma unroll
-          for (int ai = 1; ai < RA; ++ai)
+          for (int ai = 1; ai < RB; ++ai)
             if (ai == ab) v = a[ai][bj];
-          sh.stage[buf][ty & 1][tx + 16 * bj] = v;
+          if (tx + kGjCW * bj < N) sh.stage[buf][ty & 1][tx + kGjCW * bj] = v;
         }
       }
-    } else if (s + 1 < STEPS) {
-      // rows k+2, k+3 as staged during step s-1 (slot (s+1) & 1), step s
-      // applied, then step s+1 published
+    } else if (pivot && s + 1 < STEPS) {
+      // step s+1's pivot block first (seven broadcast loads, two FMAs each),
+      // then rows k+2, k+3 as staged during step s-1 (slot (s+1) & 1) with
+      // step s applied
       const int k2 = k + 2;
       const double2 ua = sh.u[buf][k2], ub = sh.u[buf][k2 + 1];
+      const double2 wa = sh.w[buf][k2], wb = sh.w[buf][k2 + 1];
+      const double* st0 = sh.stage[buf ^ 1][0];
+      const double* st1 = sh.stage[buf ^ 1][1];
+      const double pa = fma(-ua.x, wa.x, fma(-ua.y, wa.y, st0[k2]));
+      const double pb = fma(-ua.x, wb.x, fma(-ua.y, wb.y, st0[k2 + 1]));
+      const double pd = fma(-ub.x, wb.x, fma(-ub.y, wb.y, st1[k2 + 1]));
 #pragma unroll
       for (int c = 0; c < CP; ++c) {
         const int j = lane + 32 * c;
         if (j < N) {
           const double2 wv = sh.w[buf][j];
-          r0[c] = fma(-ua.x, wv.x, fma(-ua.y, wv.y, sh.stage[buf ^ 1][0][j]));
-          r1[c] = fma(-ub.x, wv.x, fma(-ub.y, wv.y, sh.stage[buf ^ 1][1][j]));
+          r0[c] = fma(-ua.x, wv.x, fma(-ua.y, wv.y, st0[j]));
+          r1[c] = fma(-ub.x, wv.x, fma(-ub.y, wv.y, st1[j]));
         }
       }
-      gj2_publish<RB>(r0, r1, k2, buf ^ 1, sh);
+      gj2_publish<RB>(r0, r1, pa, pb, pd, k2, buf ^ 1, sh);
     }
     __syncthreads();
   }
@@ -303,67 +317,68 @@ __device__ bool gj_inverse(double (&a)[(RB + 1) / 2][RB], GjShared<RB>& sh) {
   // G^-1 = D G'^-1 D
   if (bulk) {
 #pragma unroll
-    for (int ai = 0; ai < RA; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
+      for (int bj = 0; bj < CB; ++bj) a[ai][bj] *= di[ai] * dj[bj];
   }
   return true;
 }
 
 // G(i, j) = prod_{m != mode} Gram_m(i, j) for this bulk thread's entries
-// (rows ty + 32a, columns tx + 16b). All loads are issued before any store
+// (rows ty + 16a, columns tx + 24b). All loads are issued before any store
 // (grams and hadam are distinct buffers).
 template <int RB>
 __device__ void load_hadamard(const double* __restrict__ grams, double* __restrict__ hadam,
                               int ndim, int mode, int R, double ridge,
-                              double (&a)[(RB + 1) / 2][RB], bool write_h) {
-  constexpr int RA = (RB + 1) / 2;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+                              double (&a)[RB][GjLayout<RB>::CB], bool write_h) {
+  constexpr int N = GjLayout<RB>::N, CB = GjLayout<RB>::CB;
+  const int t = gj_bulk_index(), ty = t / kGjCW, tx = t % kGjCW;
   const int RR = R * R;
 #pragma unroll
-  for (int ai = 0; ai < RA; ++ai)
+  for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) a[ai][bj] = 1.0;  // helpers.rs:414 starts from ones
+    for (int bj = 0; bj < CB; ++bj) a[ai][bj] = 1.0;  // helpers.rs:414 starts from ones
   for (int m = 0; m < ndim; ++m) {
     if (m == mode) continue;
     const double* g = grams + (int64_t)m * RR;
-    double v[RA][RB];
+    double v[RB][CB];
 #pragma unroll
-    for (int ai = 0; ai < RA; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) {
-        const int i = ty + 32 * ai, j = tx + 16 * bj;
+      for (int bj = 0; bj < CB; ++bj) {
+        const int i = ty + 16 * ai, j = tx + kGjCW * bj;
         v[ai][bj] = (i < R && j < R) ? __ldg(g + (i <= j ? i * R + j : j * R + i)) : 1.0;
       }
 #pragma unroll
-    for (int ai = 0; ai < RA; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) a[ai][bj] *= v[ai][bj];
+      for (int bj = 0; bj < CB; ++bj) a[ai][bj] *= v[ai][bj];
   }
 #pragma unroll
-  for (int ai = 0; ai < RA; ++ai)
+  for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj) {
-      const int i = ty + 32 * ai, j = tx + 16 * bj;
+    for (int bj = 0; bj < CB; ++bj) {
+      const int i = ty + 16 * ai, j = tx + kGjCW * bj;
       if (i < R && j < R) {
         if (write_h) hadam[(int64_t)mode * RR + i * R + j] = a[ai][bj];
         if (i == j) a[ai][bj] += ridge;
       } else {
-        a[ai][bj] = (i == j) ? 1.0 : 0.0;  // padding: identity block, inverted harmlessly
+        // padding: identity block, inverted harmlessly (columns >= N unused)
+        a[ai][bj] = (i == j && j < N) ? 1.0 : 0.0;
       }
     }
 }
 
 // a += l2 * I on this bulk thread's entries (the ridge of cp_als_constrained)
 template <int RB>
-__device__ __forceinline__ void add_diagonal(double (&a)[(RB + 1) / 2][RB], int R, double l2) {
-  constexpr int RA = (RB + 1) / 2;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+__device__ __forceinline__ void add_diagonal(double (&a)[RB][GjLayout<RB>::CB], int R, double l2) {
+  constexpr int CB = GjLayout<RB>::CB;
+  const int t = gj_bulk_index(), ty = t / kGjCW, tx = t % kGjCW;
 #pragma unroll
-  for (int ai = 0; ai < RA; ++ai)
+  for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-    for (int bj = 0; bj < RB; ++bj)
-      if (ty + 32 * ai == tx + 16 * bj && ty + 32 * ai < R) a[ai][bj] += l2;
+    for (int bj = 0; bj < CB; ++bj)
+      if (ty + 16 * ai == tx + kGjCW * bj && ty + 16 * ai < R) a[ai][bj] += l2;
 }
 
 // fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
@@ -443,10 +458,10 @@ __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int n
     if (*(volatile int*)&st->done) return;
   }
   const int RR = R * R;
-  // threads 0..511 hold the matrix, 32 x 16 grid; warp 16 is the inverse's
+  // the bulk warps hold the matrix (16 x 24 grid); warp 0 is the inverse's
   // pivot warp
-  const bool bulk = threadIdx.x < kGjBulk;
-  double a[(RB + 1) / 2][RB];
+  const bool bulk = gj_bulk();
+  double a[RB][GjLayout<RB>::CB];
   if (bulk) {
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
     if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
@@ -493,13 +508,13 @@ __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int n
     }
     return;
   }
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   if (bulk) {
+    const int t = gj_bulk_index(), ty = t / kGjCW, tx = t % kGjCW;
 #pragma unroll
-    for (int ai = 0; ai < (RB + 1) / 2; ++ai)
+    for (int ai = 0; ai < RB; ++ai)
 #pragma unroll
-      for (int bj = 0; bj < RB; ++bj) {
-        const int i = ty + 32 * ai, j = tx + 16 * bj;
+      for (int bj = 0; bj < GjLayout<RB>::CB; ++bj) {
+        const int i = ty + 16 * ai, j = tx + kGjCW * bj;
         if (i < R && j < R) b.ginv[i * R + j] = a[ai][bj];
       }
   }
