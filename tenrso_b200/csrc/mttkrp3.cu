@@ -21,11 +21,11 @@
 // with the 128-byte swizzle, rows 0..n_pad-1 the hi halves of U's columns and
 // rows n_pad..2 n_pad-1 the lo halves. The CP-ALS solve that updates U writes
 // it, so a CTA fetches it with one bulk copy instead of converting U itself.
-// Per 16-wide k-slice two MMAs run:
-//   D[:, 0:2n_pad]     = Xhi . [Uhi | Ulo]   (N = 2 n_pad)
-//   D[:, n_pad:2n_pad] += Xlo . Uhi          (N = n_pad)
-// so D holds hi.hi in its first half and the two correction products in its
-// second (the lo.lo term, relative size 2^-32, is dropped).
+// Per 16-wide k-slice two MMAs of N = 2 n_pad accumulate into one TMEM
+// accumulator:
+//   D += Xhi . [Uhi | Ulo],  D += Xlo . [Uhi | Ulo]
+// so D[:, n] + D[:, n_pad + n] = (Xhi + Xlo) . (Uhi + Ulo) column n: every
+// product of the split values, the lo.lo term included.
 //
 // Per CTA: one 128-row M tile and a range of whole runs (split-K).
 //   warp 0      TMA producer: the A tiles of every run (hi and lo, 128-byte
@@ -40,6 +40,8 @@
 // Every mbarrier wait is bounded; a wait that runs out raises DS_TIMEOUT and
 // the CTA drains its copies, waits for its MMAs and frees TMEM before exiting.
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 #include "mttkrp.cuh"
 #include "sm100.cuh"
@@ -214,8 +216,7 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t amaj = p.mode == 2 ? (1u << 15) : 0u;  // transpose A: MN-major
-      const uint32_t idesc1 = idesc_bf16_f32(M3_BM, 2 * p.n_pad) | amaj;
-      const uint32_t idesc2 = idesc_bf16_f32(M3_BM, p.n_pad) | amaj;
+      const uint32_t idesc = idesc_bf16_f32(M3_BM, 2 * p.n_pad) | amaj;
       bool ok = nruns == 0 || m3_wait(b_full, 0, abort_flag, p.wait_budget);
       for (int r = 0; ok && r < nruns; ++r) {
         const int b = r & 1;
@@ -251,8 +252,11 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
             }
             const uint64_t db = desc_sw128_kmajor(bt + kk * 32u);
             const uint32_t first = (sp == 0 && kk == 0) ? 0u : 1u;
-            mma_bf16(acc, dah, db, idesc1, first);                           // hi.[hi|lo]
-            mma_bf16(acc + (uint32_t)p.n_pad, dal, db, idesc2, 1u);          // + lo.hi
+            // both products accumulate into the whole accumulator: an MMA into
+            // a column range that only overlaps the previous one serialises the
+            // tensor pipe, one into the same range pipelines
+            mma_bf16(acc, dah, db, idesc, first);  // Xhi . [Uhi | Ulo]
+            mma_bf16(acc, dal, db, idesc, 1u);     // + Xlo . [Uhi | Ulo]
           }
           mma_commit(&empty[s]);
         }
@@ -486,7 +490,35 @@ EncodeTiledFn3 encode_fn() {
 }
 
 // X as (K, J, I) with the box of `mode`: (64, 1, 128), (64, 128, 1) or (64, 64, 1).
+int encode_map3(CUtensorMap* map, const __nv_bfloat16* base, const Dense3& d, int mode);
+
+// Encoded maps are cached by (base, sizes, mode): encoding is a driver call of
+// a few microseconds, which a timed or repeated launch should not pay again.
 int make_map3(CUtensorMap* map, const __nv_bfloat16* base, const Dense3& d, int mode) {
+  struct Entry {
+    const void* base;
+    int64_t I, J, K;
+    int mode;
+    CUtensorMap map;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> cache;  // small, most recent last
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+      if (e.base == base && e.I == d.I && e.J == d.J && e.K == d.K && e.mode == mode) {
+        *map = e.map;
+        return TSR_OK;
+      }
+  }
+  TSR_TRY(encode_map3(map, base, d, mode));
+  std::lock_guard<std::mutex> lock(mu);
+  if (cache.size() >= 24) cache.erase(cache.begin());
+  cache.push_back(Entry{base, d.I, d.J, d.K, mode, *map});
+  return TSR_OK;
+}
+
+int encode_map3(CUtensorMap* map, const __nv_bfloat16* base, const Dense3& d, int mode) {
   EncodeTiledFn3 enc = encode_fn();
   if (!enc) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled unavailable");
   if (((uintptr_t)base & 15) || (d.K * 2) % 16)

@@ -46,11 +46,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait: returns false when the budget (cycles) runs out or *abort is
 // raised by another thread of the CTA.
+// The abort flag is read every 64 polls: a spinning thread's shared-memory
+// loads take bandwidth from the tensor core's operand reads.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile int* abort, long long budget) {
   long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (*abort) return false;
+  for (uint32_t n = 0; !mbar_try_wait(bar, parity); ++n) {
+    if ((n & 63u) == 63u && *abort) return false;
     if (clock64() - t0 > budget) return false;
   }
   return true;
