@@ -230,6 +230,22 @@ int tsr_cp_als_constrained_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim
                                    double time_limit_s, float* d_out_factors,
                                    tsr_cp_info* info);
 
+/* cp_als_accelerated (crates/tenrso-decomp/src/cp/advanced.rs:51-213): the
+ * CP-ALS sweep with the line search of line_search_cp (cp/helpers.rs:130-189)
+ * and the adaptive extrapolation from the second iteration on. Arguments as
+ * tsr_cp_als_f32; tol must lie in (0, 1) (TSR_E_INVALID_TOL otherwise), rank 0
+ * is TSR_E_INVALID_RANK. The result has no weights; info->ridge_used reports
+ * the solve's ridge retry. */
+int tsr_cp_als_accelerated_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                               int64_t rank, int max_iters, double tol,
+                               const float* init_factors, uint64_t seed, int precision,
+                               double time_limit_s, float* out_factors, tsr_cp_info* info);
+/* Device-resident form; arguments as tsr_cp_als_dev_f32. */
+int tsr_cp_als_accelerated_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim,
+                                   const int64_t* shape, int64_t rank, int max_iters, double tol,
+                                   const float* d_init, int precision, double time_limit_s,
+                                   float* d_out_factors, tsr_cp_info* info);
+
 /* ---- sparse: crates/tenrso-sparse --------------------------------------
  * COO entries are `indices` (nnz x ndim, row-major int64) and `values`
  * (nnz float32). Validation follows CooTensor::new (coo.rs:101-149). */

@@ -259,6 +259,90 @@ def coo_mttkrp(idx, vals, shape, factors, mode):
     return out
 
 
+def compute_fit(X: np.ndarray, factors, xnorm_sq: float) -> float:
+    """Restated ``compute_fit`` (cp/helpers.rs:513-530) in FP64:
+    ||Xhat||^2 from the Hadamard of the factor Grams (helpers.rs:533-556),
+    <X, Xhat> from the mode-0 MTTKRP of the factors (helpers.rs:558-579)."""
+    R = factors[0].shape[1]
+    H = np.ones((R, R))
+    for f in factors:
+        H *= gram(f)
+    inner = float(np.sum(mttkrp(X, factors, 0) * factors[0]))
+    err = np.sqrt(max(xnorm_sq + float(H.sum()) - 2.0 * inner, 0.0))
+    return min(max(1.0 - err / np.sqrt(xnorm_sq), 0.0), 1.0)
+
+
+def cp_als_accelerated(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
+                       trace=None):
+    """Restated ``cp_als_accelerated`` (cp/advanced.rs:51-213) in FP64 from
+    injected factors: per mode the MTTKRP, Gram-Hadamard and solve of
+    cp_als, then ``line_search_cp`` (helpers.rs:130-189: the fit of
+    prev + a (new - prev) for a in 0.25, 0.5, 0.75, 1, 1.25, the first best
+    kept), then from the second iteration on the extrapolation
+    new += a_ls * alpha * (new - prev), prev being the factor before the
+    previous update. After each sweep: the fit, the adaptive alpha (x1.05 up
+    to 0.9 when the fit rose, else x0.7 down to 0.1 and one more oscillation;
+    stop at > 5 oscillations after iteration 10), and the relative-change
+    tolerance |fit - prev| / (|prev| + 1e-10) < tol. Returns (factors, info).
+    With `trace` a list, each line search appends (iteration, mode, chosen a,
+    the five trial fits)."""
+    if rank == 0:
+        raise ValueError(f"Invalid rank: {rank}")
+    if not (0.0 < tol < 1.0):
+        raise ValueError(f"Invalid tolerance: {tol}")
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    U = [np.array(f, dtype=np.float64) for f in init_factors]
+    prev = [f.copy() for f in U]
+    alpha, alpha_max, alpha_min = 0.5, 0.9, 0.1
+    xn = float(np.sum(X * X))
+    prev_fit, fit, osc, change, reason = 0.0, 0.0, 0, 0.0, "MaxIterations"
+    hist, iters = [], 0
+    alphas = (0.25, 0.5, 0.75, 1.0, 1.25)
+    for it in range(max_iters):
+        iters = it + 1
+        for n in range(X.ndim):
+            M = mttkrp(X, U, n)
+            G = np.ones((rank, rank))
+            for m in range(X.ndim):
+                if m != n:
+                    G *= gram(U[m])
+            new = solve(M, G)
+            best_a, best_fit, fits = 1.0, -np.inf, []
+            for a in alphas:
+                test = list(U)
+                test[n] = prev[n] + a * (new - prev[n])
+                f = compute_fit(X, test, xn)
+                fits.append(f)
+                if f > best_fit:
+                    best_fit, best_a = f, a
+            if trace is not None:
+                trace.append((it, n, best_a, fits))
+            if it > 0:
+                new = new + best_a * alpha * (new - prev[n])
+            prev[n] = U[n].copy()
+            U[n] = new
+        fit = compute_fit(X, U, xn)
+        hist.append(fit)
+        if it > 0:
+            if fit > prev_fit:
+                alpha = min(alpha * 1.05, alpha_max)
+            else:
+                alpha = max(alpha * 0.7, alpha_min)
+                osc += 1
+                if osc > 5 and it > 10:
+                    reason = "Oscillation"
+                    break
+        if it > 0:
+            change = abs(fit - prev_fit)
+            if change / (abs(prev_fit) + 1e-10) < tol:
+                reason = "FitTolerance"
+                break
+        prev_fit = fit
+    info = dict(fit=fit, iters=iters, reason=reason, oscillation_count=osc, oscillated=osc > 0,
+                final_fit_change=change, fit_history=np.asarray(hist))
+    return U, info
+
+
 def cp_als_coo(idx, vals, shape, rank: int, max_iters: int, tol: float, init_factors):
     """CP-ALS of a sparse tensor given as COO, in FP64: the loop of
     ``cp_als`` (cp/core.rs:59-182; mode order, solve_least_squares restated

@@ -11,6 +11,8 @@ from .dense import (  # noqa: F401
     CpDecomp,
     cp_als,
     cp_als_dev,
+    cp_als_accelerated,
+    cp_als_accelerated_dev,
     default_context,
     gram_inverse,
     khatri_rao,

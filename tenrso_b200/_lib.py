@@ -74,6 +74,11 @@ SIGNATURES = {
     "tsr_cp_als_constrained_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
                                                  C.POINTER(CpConstraintsC), C.c_int, C.c_double,
                                                  P, C.POINTER(CpInfo)]),
+    "tsr_cp_als_accelerated_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
+                                             C.c_uint64, C.c_int, C.c_double, P,
+                                             C.POINTER(CpInfo)]),
+    "tsr_cp_als_accelerated_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
+                                                 C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
     "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_coo_deduplicate_f32": (C.c_int, [P, P, P, I64, C.c_int, P, PI64]),
     "tsr_csf_from_coo_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, P, P, P, P]),

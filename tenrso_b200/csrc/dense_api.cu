@@ -646,6 +646,7 @@ void init_kernel_attributes() {
   init_adjoint_attributes();
   init_csf_attributes();
   init_batched_attributes();
+  init_accel_attributes();
   done_mask |= 1ull << dev;
 }
 

@@ -301,6 +301,61 @@ def cp_als_dev(d_tensor: int, shape, rank: int, max_iters: int, tol: float, d_in
     return float(info.fit), int(info.iters), _info_to(info, hist)
 
 
+def cp_als_accelerated(tensor, rank: int, max_iters: int, tol: float, init="random",
+                       time_limit: Optional[float] = None, precision="fp32", seed: int = 0,
+                       ctx: Optional[Context] = None) -> CpDecomp:
+    """cp_als_accelerated (cp/advanced.rs:51-213): the CP-ALS sweep with the
+    five-step line search of line_search_cp (cp/helpers.rs:130-189) and the
+    adaptive extrapolation U_n = U_new + a_ls * alpha * (U_new - U_prev) from
+    the second iteration on. tol must lie in (0, 1). init as in cp_als."""
+    if rank == 0:
+        raise TenrsoError(5, f"Invalid rank: {rank}")
+    if not 0.0 < tol < 1.0:
+        raise TenrsoError(6, f"Invalid tolerance: {tol}")
+    t = _f32(tensor)
+    shape = _i64(t.shape)
+    total = int(sum(n * rank for n in t.shape))
+    out = np.zeros(max(total, 1), dtype=np.float32)
+    if isinstance(init, str):
+        if init.lower() != "random":
+            raise ValueError("only InitStrategy::Random or injected factors are supported")
+        init_ptr = None
+    else:
+        flat = np.concatenate([_f32(f).ravel() for f in init])
+        if flat.size != total:
+            raise ValueError("initial factors do not match shape x rank")
+        init_ptr = _ptr(flat)
+    hist = np.zeros(max(max_iters, 1), dtype=np.float64)
+    info = CpInfo()
+    info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))
+    check(_lib.load().tsr_cp_als_accelerated_f32(
+        _ctx_handle(ctx), _ptr(t), t.ndim, _ptr(shape), rank, max_iters, float(tol), init_ptr,
+        seed, _prec(precision), -1.0 if time_limit is None else float(time_limit), _ptr(out),
+        C.byref(info)))
+    factors, off = [], 0
+    for n in t.shape:
+        factors.append(out[off:off + n * rank].reshape(n, rank).copy())
+        off += n * rank
+    return CpDecomp(factors=factors, weights=None, fit=float(info.fit), iters=int(info.iters),
+                    convergence=_info_to(info, hist), ridge_used=bool(info.ridge_used))
+
+
+def cp_als_accelerated_dev(d_tensor: int, shape, rank: int, max_iters: int, tol: float,
+                           d_init: int, d_out: int, precision="fp32",
+                           time_limit: Optional[float] = None, ctx: Optional[Context] = None):
+    """Device-resident cp_als_accelerated on raw device pointers; returns
+    (fit, iters, ConvergenceInfo). Factors are written to d_out (concatenated)."""
+    shp = _i64(shape)
+    hist = np.zeros(max(max_iters, 1), dtype=np.float64)
+    info = CpInfo()
+    info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))
+    check(_lib.load().tsr_cp_als_accelerated_dev_f32(
+        _ctx_handle(ctx), C.c_void_p(d_tensor), len(shape), _ptr(shp), rank, max_iters,
+        float(tol), C.c_void_p(d_init), _prec(precision),
+        -1.0 if time_limit is None else float(time_limit), C.c_void_p(d_out), C.byref(info)))
+    return float(info.fit), int(info.iters), _info_to(info, hist)
+
+
 def profile_mttkrp_dev(d_tensor: int, shape, d_factors: Sequence[int], rank: int, mode: int,
                        precision="bf16x3", iters: int = 10, flush_l2: bool = True,
                        ctx: Optional[Context] = None):

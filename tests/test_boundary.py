@@ -129,3 +129,25 @@ def test_batched_validation():
         tb.BatchedCpAls([Y], [17])
     with pytest.raises(ValueError, match="3-way"):
         tb.BatchedCpAls([np.ones((3, 3), np.float32)], [1])
+
+
+def test_cp_als_accelerated_validation():
+    """advanced.rs:71-77 in the Python mirror and in the C ABI itself (the C
+    checks run before the context is touched, so a NULL context is fine)."""
+    X = np.ones((3, 4, 5), dtype=np.float32)
+    with pytest.raises(tb.TenrsoError, match="Invalid rank: 0"):
+        tb.cp_als_accelerated(X, 0, 5, 1e-4)
+    for tol in (0.0, 1.0, -0.1):
+        with pytest.raises(tb.TenrsoError, match="Invalid tolerance"):
+            tb.cp_als_accelerated(X, 2, 5, tol)
+    lib = _lib.load()
+    shape = np.array(X.shape, dtype=np.int64)
+    out = np.zeros(12 * 4, dtype=np.float32)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = lib.tsr_cp_als_accelerated_f32(None, ptr(X), 3, ptr(shape), 0, 5, 1e-4, None, 0, 0, -1.0,
+                                        ptr(out), None)
+    assert rc == 5 and b"Invalid rank: 0" in lib.tsr_last_error()
+    for tol in (0.0, 1.0):
+        rc = lib.tsr_cp_als_accelerated_f32(None, ptr(X), 3, ptr(shape), 2, 5, tol, None, 0, 0,
+                                            -1.0, ptr(out), None)
+        assert rc == 6 and b"Invalid tolerance" in lib.tsr_last_error()

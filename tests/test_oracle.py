@@ -220,3 +220,66 @@ def test_cp_als_coo_matches_dense_oracle(orc):
     _, a = orc.cp_als_coo(nz, X[tuple(nz.T)], shape, 4, 8, 0.0, init)
     _, b = orc.cp_als(X.astype(np.float64), 4, 8, 0.0, [f.astype(np.float64) for f in init])
     assert np.abs(a["fit_history"] - b["fit_history"]).max() <= 1e-12
+
+
+def test_accelerated_first_sweep_is_cp_als(orc):
+    """No extrapolation in the first iteration (advanced.rs:137-147) and the
+    line search picks a = 1 (the solve minimises the error along the line), so
+    the first fit of cp_als_accelerated is cp_als's."""
+    X = synth.uniform(0xC1, 7, (64, 64, 64))
+    init = [f.astype(np.float64) for f in synth.init_factors((64, 64, 64), 8, 0xC1)]
+    trace = []
+    _, acc = orc.cp_als_accelerated(X, 8, 3, 1e-9, init, trace=trace)
+    _, std = orc.cp_als(X, 8, 1, 0.0, init)
+    assert abs(acc["fit_history"][0] - std["fit_history"][0]) <= 1e-12
+    assert all(a == 1.0 for _, _, a, _ in trace)
+    with pytest.raises(ValueError):
+        orc.cp_als_accelerated(X, 8, 3, 0.0, init)
+    with pytest.raises(ValueError):
+        orc.cp_als_accelerated(X, 0, 3, 0.5, init)
+
+
+@pytest.mark.parametrize("shape,R", [((12, 10, 9), 5), ((7, 6, 5, 4), 3)])
+def test_line_search_closed_form(orc, shape, R):
+    """The device evaluates line_search_cp's trial fits (helpers.rs:130-189)
+    from five sums: <M, prev>, <M, d>, <G, prev'prev>, <G, prev'd>, <G, d'd>
+    with d = U_new - prev, M the mode's MTTKRP and G the Hadamard of the other
+    Grams. They equal compute_fit of the trial factors."""
+    rng = np.random.default_rng(3)
+    X = rng.random(shape)
+    U = [rng.random((n, R)) for n in shape]
+    prev = [rng.random((n, R)) for n in shape]
+    xn = float(np.sum(X * X))
+    for n in range(len(shape)):
+        M = orc.mttkrp(X, U, n)
+        G = np.ones((R, R))
+        for m in range(len(shape)):
+            if m != n:
+                G *= orc.gram(U[m])
+        new = orc.solve(M, G)
+        d = new - prev[n]
+        s0, s1 = np.sum(M * prev[n]), np.sum(M * d)
+        q1 = np.sum(G * (prev[n].T @ prev[n]))
+        q2 = np.sum(G * (prev[n].T @ d))
+        q3 = np.sum(G * (d.T @ d))
+        for a in (0.25, 0.5, 0.75, 1.0, 1.25):
+            test = list(U)
+            test[n] = prev[n] + a * d
+            lit = orc.compute_fit(X, test, xn)
+            err = np.sqrt(max(xn + q1 + 2 * a * q2 + a * a * q3 - 2 * (s0 + a * s1), 0.0))
+            closed = min(max(1.0 - err / np.sqrt(xn), 0.0), 1.0)
+            assert abs(lit - closed) <= 1e-12, (n, a, lit, closed)
+
+
+def test_oracle_reproduces_c2_accel_fixture(orc):
+    """The committed FP64 history of cp_als_accelerated on the 256^3 rank-64
+    workload (tests/golden/make_c2_accel.py): the first two sweeps re-derived."""
+    import json
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "c2_accel_fp64.json")) as f:
+        ref = json.load(f)
+    X, _ = synth.dense_lowrank((256, 256, 256), 64, seed=0xC2, dist="uniform", noise=0.005)
+    init = [f.astype(np.float64) for f in synth.init_factors((256, 256, 256), 64, 0xC2)]
+    _, info = orc.cp_als_accelerated(X.astype(np.float64), 64, 2, 1e-9, init)
+    assert np.allclose(info["fit_history"], ref["fp64_fit_history"][:2], rtol=0, atol=1e-12)
