@@ -46,7 +46,8 @@ typedef enum tsr_status {
   TSR_E_SHAPE = 16,          /* cp/types.rs:24 CpError::ShapeMismatch / coo.rs errors */
   TSR_E_INDEX_OOB = 17,      /* coo.rs:130-137 CooError::IndexOutOfBounds */
   TSR_E_NONNEG_VIOLATION = 18, /* cp/types.rs:30-31 CpError::NonnegativeViolation */
-  TSR_E_INVALID_REGULARIZATION = 19 /* cp/types.rs:33-34 CpError::InvalidRegularization */
+  TSR_E_INVALID_REGULARIZATION = 19, /* cp/types.rs:33-34 CpError::InvalidRegularization */
+  TSR_E_BLOCK_SHAPE = 20     /* hicoo.rs:43-44 HiCooError::InvalidBlockShape */
 } tsr_status;
 
 /* Arithmetic of the dense MTTKRP. FP32: IEEE fp32 FMA on the SIMT pipes.
@@ -305,6 +306,33 @@ int tsr_cp_als_sparse_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int 
 int tsr_cp_als_sparse_dev_f32(tsr_ctx* ctx, const tsr_sparse* sp, int64_t rank, int max_iters,
                               double tol, const float* d_init, double time_limit_s,
                               float* d_out_factors, tsr_cp_info* info);
+
+/* ---- HiCOO: crates/tenrso-sparse/src/hicoo.rs ---------------------------
+ * HiCooTensor::from_coo (hicoo.rs:118-203): entries split into block
+ * coordinates i / b and local coordinates i % b, stably sorted by block
+ * coordinate; nothing merged. Block sides up to 256 (u8 local coordinates on
+ * the device; larger sides give TSR_E_UNSUPPORTED). Errors: a block_shape
+ * whose length differs from ndim or that holds a zero is TSR_E_BLOCK_SHAPE
+ * with hicoo.rs's messages; shape and index checks as CooTensor::new. */
+typedef struct tsr_hicoo tsr_hicoo;
+int tsr_hicoo_create_f32(tsr_ctx* ctx, const int64_t* indices, const float* values, int64_t nnz,
+                         int ndim, const int64_t* shape, const int64_t* block_shape,
+                         int n_block_shape, tsr_hicoo** out);
+int tsr_hicoo_destroy(tsr_hicoo* h);
+/* nnz() and num_blocks() (hicoo.rs:229-238). */
+int tsr_hicoo_info(const tsr_hicoo* h, int64_t* nnz, int64_t* num_blocks);
+/* block_coords (num_blocks x ndim), block_ptrs (num_blocks + 1), local_coords
+ * (nnz x ndim) and values (hicoo.rs:249-271) copied to host arrays; any may
+ * be NULL. */
+int tsr_hicoo_export(tsr_ctx* ctx, const tsr_hicoo* h, int64_t* block_coords,
+                     int64_t* block_ptrs, int64_t* local_coords, float* values);
+/* Sparse MTTKRP on the HiCOO layout (no tenrso implementation; hicoo.rs:30-34
+ * names it): out (shape[mode] x rank) = sum over entries of
+ * v * prod_{m != mode} U_m[i_m, :]. Factors are host arrays (I_m x rank). */
+int tsr_mttkrp_hicoo_f32(tsr_ctx* ctx, const tsr_hicoo* h, const float* const* factors,
+                         int64_t rank, int mode, float* out);
+int tsr_mttkrp_hicoo_dev_f32(tsr_ctx* ctx, const tsr_hicoo* h, const float* const* d_factors,
+                             int64_t rank, int mode, float* d_out);
 
 /* ---- CP reconstruction and its adjoint ----------------------------------
  * tenrso_kernels::cp_reconstruct (crates/tenrso-kernels/src/outer.rs:223-274):

@@ -246,6 +246,29 @@ def csf_from_coo(idx: np.ndarray, vals: np.ndarray, mode_order):
     return fp, fi, vout[:nv].copy()
 
 
+def hicoo_from_coo(idx, vals, block_shape):
+    """Restated ``HiCooTensor::from_coo`` (hicoo.rs:118-203): block
+    coordinates i // b and local coordinates i % b, a stable sort by block
+    coordinate (lexicographic, mode 0 first), cumulative block pointers.
+    Returns (block_coords, block_ptrs, local_coords, values)."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64).reshape(len(vals), -1)
+    vals = np.ascontiguousarray(vals, dtype=np.float32)
+    bs = np.asarray(block_shape, dtype=np.int64)
+    if len(vals) == 0:
+        return (np.zeros((0, len(bs)), np.int64), np.zeros(1, np.int64),
+                np.zeros((0, len(bs)), np.int64), vals.copy())
+    blk = idx // bs
+    loc = idx % bs
+    # np.lexsort is stable; its last key is the primary one
+    order = np.lexsort(tuple(blk[:, m] for m in range(blk.shape[1] - 1, -1, -1)))
+    blk, loc, v = blk[order], loc[order], vals[order]
+    new = np.ones(len(v), bool)
+    new[1:] = np.any(blk[1:] != blk[:-1], axis=1)
+    starts = np.flatnonzero(new)
+    ptrs = np.append(starts, len(v)).astype(np.int64)
+    return blk[starts], ptrs, loc, v
+
+
 def coo_mttkrp(idx, vals, shape, factors, mode):
     """Sparse MTTKRP definition (no reference implementation), FP64."""
     idx = np.ascontiguousarray(idx, dtype=np.int64)

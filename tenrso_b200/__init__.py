@@ -31,6 +31,7 @@ from .sparse import (  # noqa: F401
     CooTensor,
     CsfError,
     CsfTensor,
+    HiCooTensor,
     SparseTensor,
     coo_deduplicate_dev,
     synth_zipf_coo_dev,

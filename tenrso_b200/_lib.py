@@ -79,6 +79,12 @@ SIGNATURES = {
                                              C.POINTER(CpInfo)]),
     "tsr_cp_als_accelerated_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P,
                                                  C.c_int, C.c_double, P, C.POINTER(CpInfo)]),
+    "tsr_hicoo_create_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, C.POINTER(P)]),
+    "tsr_hicoo_destroy": (C.c_int, [P]),
+    "tsr_hicoo_info": (C.c_int, [P, PI64, PI64]),
+    "tsr_hicoo_export": (C.c_int, [P, P, P, P, P, P]),
+    "tsr_mttkrp_hicoo_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
+    "tsr_mttkrp_hicoo_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_coo_deduplicate_f32": (C.c_int, [P, P, P, I64, C.c_int, P, PI64]),
     "tsr_csf_from_coo_f32": (C.c_int, [P, P, P, I64, C.c_int, P, P, C.c_int, P, P, P, P]),
@@ -145,6 +151,7 @@ STATUS = {
     11: "TSR_E_NEED_2_FACTORS", 12: "TSR_E_TILE_SIZE", 13: "TSR_E_MODE_ORDER",
     14: "TSR_E_UNSUPPORTED", 15: "TSR_E_COLS_MISMATCH", 16: "TSR_E_SHAPE",
     17: "TSR_E_INDEX_OOB", 18: "TSR_E_NONNEG_VIOLATION", 19: "TSR_E_INVALID_REGULARIZATION",
+    20: "TSR_E_BLOCK_SHAPE",
 }
 
 

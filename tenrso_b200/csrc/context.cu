@@ -385,6 +385,9 @@ const char* tsr_status_string(int s) {
     case TSR_E_COLS_MISMATCH: return "number of columns must match";
     case TSR_E_SHAPE: return "shape mismatch";
     case TSR_E_INDEX_OOB: return "index out of bounds";
+    case TSR_E_NONNEG_VIOLATION: return "nonnegative constraint violated";
+    case TSR_E_INVALID_REGULARIZATION: return "invalid regularization parameter";
+    case TSR_E_BLOCK_SHAPE: return "invalid block shape";
     default: return "unknown status";
   }
 }

@@ -622,6 +622,11 @@ void launch_csf3_slot(tsr_ctx* ctx, cudaStream_t s, const Csf3Args& a) {
 
 }  // namespace
 
+int coo_check_shape(int ndim, const int64_t* shape) { return check_shape(ndim, shape); }
+int coo_check_bounds(const int64_t* idx, int64_t nnz, int ndim, const int64_t* shape) {
+  return check_host_bounds(idx, nnz, ndim, shape);
+}
+
 void init_csf_attributes() {}  // the CSF kernels use no dynamic shared memory
 
 int launch_csf_accumulate(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp,

@@ -46,5 +46,9 @@ int launch_mttkrp_csf(tsr_ctx* ctx, cudaStream_t s, const tsr_sparse* sp, const 
                       int R, int mode, float* d_out, double* d_acc);
 // Shared-memory limits of the CSF kernels (once per process, before capture).
 void init_csf_attributes();
+void init_hicoo_attributes();
+// CooTensor::new's shape and index checks (coo.rs:101-149), tenrso's wording.
+int coo_check_shape(int ndim, const int64_t* shape);
+int coo_check_bounds(const int64_t* idx, int64_t nnz, int ndim, const int64_t* shape);
 
 }  // namespace tsr

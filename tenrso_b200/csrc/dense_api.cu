@@ -647,6 +647,7 @@ void init_kernel_attributes() {
   init_csf_attributes();
   init_batched_attributes();
   init_accel_attributes();
+  init_hicoo_attributes();
   done_mask |= 1ull << dev;
 }
 

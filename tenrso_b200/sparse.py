@@ -2,6 +2,7 @@
 
   CooTensor (new/sort/deduplicate/to_dense)   crates/tenrso-sparse/src/coo.rs:73-347
   CsfTensor.from_coo + accessors              crates/tenrso-sparse/src/csf.rs:137-331
+  HiCooTensor.from_coo + accessors + MTTKRP    crates/tenrso-sparse/src/hicoo.rs:79-359
   SparseTensor: device-resident per-mode CSF for the sparse MTTKRP and sparse
   CP-ALS, which tenrso does not implement (csf.rs:42 only names MTTKRP).
 
@@ -189,6 +190,140 @@ class CsfTensor:
         if nd > 1:
             idx[:, self._mode_order[-1]] = self._fids[-1]
         return CooTensor(idx, self._vals, self._shape)
+
+
+class HiCooTensor:
+    """HiCooTensor (hicoo.rs:79-359): block coordinates, cumulative block
+    pointers, within-block local coordinates and values, built on the device
+    by from_coo. The device copy stays attached for the HiCOO MTTKRP."""
+
+    def __init__(self, handle, ctx, shape, block_shape, block_coords, block_ptrs, local_coords,
+                 values):
+        self._h = handle
+        self._ctx = ctx
+        self._shape = list(shape)
+        self._block_shape = list(block_shape)
+        self._block_coords = block_coords
+        self._block_ptrs = block_ptrs
+        self._local = local_coords
+        self._values = values
+
+    @classmethod
+    def from_coo(cls, coo: CooTensor, block_shape: Sequence[int], ctx=None) -> "HiCooTensor":
+        """hicoo.rs:118-203. Raises TenrsoError (TSR_E_BLOCK_SHAPE) with
+        hicoo.rs's messages for a block_shape of the wrong length or with a
+        zero."""
+        ndim, nnz = coo.rank(), coo.nnz()
+        bs = list(block_shape)
+        if len(bs) != ndim:
+            raise TenrsoError(20, f"Invalid block shape: block_shape length {len(bs)} != "
+                                  f"ndim {ndim}")
+        if 0 in bs:
+            raise TenrsoError(20, "Invalid block shape: block_shape cannot contain zeros")
+        lib = _lib.load()
+        h = C.c_void_p()
+        check(lib.tsr_hicoo_create_f32(_ctx_handle(ctx), _ptr(coo.indices()), _ptr(coo.values()),
+                                       nnz, ndim, _ptr(_i64(coo.shape())),
+                                       _ptr(_i64(bs or [0])), len(bs), C.byref(h)))
+        n, nb = C.c_int64(0), C.c_int64(0)
+        check(lib.tsr_hicoo_info(h, C.byref(n), C.byref(nb)))
+        bc = np.zeros((max(nb.value, 1), ndim), np.int64)
+        bp = np.zeros(nb.value + 1, np.int64)
+        lc = np.zeros((max(n.value, 1), ndim), np.int64)
+        vals = np.zeros(max(n.value, 1), np.float32)
+        check(lib.tsr_hicoo_export(_ctx_handle(ctx), h, _ptr(bc), _ptr(bp), _ptr(lc), _ptr(vals)))
+        return cls(h, ctx, coo.shape(), bs, bc[:nb.value], bp, lc[:n.value], vals[:n.value])
+
+    def shape(self):
+        return list(self._shape)
+
+    def block_shape(self):
+        return list(self._block_shape)
+
+    def ndim(self):
+        return len(self._shape)
+
+    def nnz(self):
+        return len(self._values)
+
+    def num_blocks(self):
+        return len(self._block_coords)
+
+    def density(self):
+        """hicoo.rs:240-247."""
+        total = float(np.prod(self._shape))
+        return self.nnz() / total if total else 0.0
+
+    def block_coords(self) -> np.ndarray:
+        return self._block_coords
+
+    def block_ptrs(self) -> np.ndarray:
+        return self._block_ptrs
+
+    def local_coords(self) -> np.ndarray:
+        return self._local
+
+    def values(self) -> np.ndarray:
+        return self._values
+
+    def _global_indices(self) -> np.ndarray:
+        counts = np.diff(self._block_ptrs)
+        blocks = np.repeat(np.arange(self.num_blocks()), counts)
+        bs = np.asarray(self._block_shape, np.int64)
+        return self._block_coords[blocks] * bs + self._local
+
+    def iter(self):
+        """(indices, value) in block-major order (hicoo.rs:298-359)."""
+        for idx, v in zip(self._global_indices(), self._values):
+            yield [int(i) for i in idx], float(v)
+
+    def to_coo(self) -> CooTensor:
+        """hicoo.rs:285-293: the entries in block-major order."""
+        return CooTensor(self._global_indices(), self._values.copy(), self._shape)
+
+    def to_dense(self) -> np.ndarray:
+        """hicoo.rs:311-321: each entry assigned in block-major order (a later
+        duplicate overwrites an earlier one)."""
+        out = np.zeros(self._shape, np.float32)
+        idx = self._global_indices()
+        if len(idx):
+            lin = np.ravel_multi_index(tuple(idx.T), self._shape)
+            # last occurrence of each position wins
+            rev = lin[::-1]
+            _, first = np.unique(rev, return_index=True)
+            keep = len(lin) - 1 - first
+            out.ravel()[lin[keep]] = self._values[keep]
+        return out
+
+    def mttkrp(self, factors, mode: int) -> np.ndarray:
+        """Sparse MTTKRP on the device's HiCOO layout (fp32 out, FP64 sums)."""
+        fs = [np.ascontiguousarray(f, dtype=np.float32) for f in factors]
+        if not 0 <= mode < self.ndim():
+            raise TenrsoError(1, f"Mode {mode} out of bounds for tensor with rank {self.ndim()}")
+        if len(fs) != self.ndim():
+            raise ValueError("one factor matrix per mode is required")
+        R = fs[0].shape[1]
+        ptrs = (C.c_void_p * len(fs))(*[f.ctypes.data for f in fs])
+        out = np.zeros((self._shape[mode], R), np.float32)
+        check(_lib.load().tsr_mttkrp_hicoo_f32(_ctx_handle(self._ctx), self._h, ptrs, R, mode,
+                                               _ptr(out)))
+        return out
+
+    def mttkrp_dev(self, d_factors, rank: int, mode: int, d_out: int):
+        ptrs = (C.c_void_p * len(d_factors))(*d_factors)
+        check(_lib.load().tsr_mttkrp_hicoo_dev_f32(_ctx_handle(self._ctx), self._h, ptrs, rank,
+                                                   mode, C.c_void_p(d_out)))
+
+    def close(self):
+        if self._h:
+            _lib.load().tsr_hicoo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def synth_zipf_coo_dev(shape, nnz: int, seed: int, d_indices: int, d_values: int,
