@@ -56,6 +56,15 @@ typedef enum tsr_status {
 typedef enum tsr_precision { TSR_PREC_FP32 = 0, TSR_PREC_BF16X3 = 1 } tsr_precision;
 
 /* cp/types.rs:319-328 ConvergenceReason */
+/* InitStrategy (crates/tenrso-decomp/src/cp/types.rs:39-59). */
+typedef enum tsr_init_strategy {
+  TSR_INIT_RANDOM = 0,
+  TSR_INIT_RANDOM_NORMAL = 1,
+  TSR_INIT_SVD = 2,
+  TSR_INIT_NNSVD = 3,
+  TSR_INIT_LEVERAGE_SCORE = 4
+} tsr_init_strategy;
+
 typedef enum tsr_reason {
   TSR_REASON_MAX_ITERATIONS = 0,
   TSR_REASON_FIT_TOLERANCE = 1,
@@ -246,6 +255,20 @@ int tsr_cp_als_accelerated_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim
                                    const int64_t* shape, int64_t rank, int max_iters, double tol,
                                    const float* d_init, int precision, double time_limit_s,
                                    float* d_out_factors, tsr_cp_info* info);
+
+/* initialize_factors (crates/tenrso-decomp/src/cp/helpers.rs:192-377) for
+ * every InitStrategy: out_factors receives the concatenated I_n x rank fp32
+ * factors. Random and RandomNormal draw from the library's seeded stream
+ * `seed` (tenrso's thread_rng cannot be seeded); Svd, Nnsvd and
+ * LeverageScore take the leading singular vectors of each unfolding (FP64 on
+ * the device, mode sizes up to 1024, each u_r oriented so that its
+ * largest-magnitude entry is positive) and pad columns past the unfolding's
+ * rank with N(0, 0.01) draws from the same seeded stream. The factors feed
+ * tsr_cp_als_f32 (and its variants) as init_factors. */
+int tsr_cp_init_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                    int64_t rank, int strategy, uint64_t seed, float* out_factors);
+int tsr_cp_init_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                        int64_t rank, int strategy, uint64_t seed, float* d_out_factors);
 
 /* ---- sparse: crates/tenrso-sparse --------------------------------------
  * COO entries are `indices` (nnz x ndim, row-major int64) and `values`

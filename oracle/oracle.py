@@ -295,6 +295,64 @@ def compute_fit(X: np.ndarray, factors, xnorm_sq: float) -> float:
     return min(max(1.0 - err / np.sqrt(xnorm_sq), 0.0), 1.0)
 
 
+INIT_STRATEGIES = ("random", "random_normal", "svd", "nnsvd", "leverage_score")
+
+
+def initialize_factors(X: np.ndarray, rank: int, strategy: str, seed: int):
+    """Restated ``initialize_factors`` (cp/helpers.rs:192-377) in FP64 with
+    the library's seeded streams in place of thread_rng: U(0,1) on stream
+    200 + n (:215-222), N(0,1) on 400 + n (:223-231), the N(0, 0.01) padding
+    of the SVD-based strategies on 500 + n. The SVD is numpy's (LAPACK gesdd)
+    thin SVD of the mode-n unfolding; each u_r is oriented so that its
+    largest-magnitude entry is positive (first such entry on ties) and v_r
+    with it. Svd :232-263, Nnsvd :264-317, LeverageScore :318-373."""
+    from tenrso_b200 import synth
+    X = np.asarray(X, dtype=np.float64)
+    out = []
+    for n, I in enumerate(X.shape):
+        if strategy == "random":
+            out.append(synth.uniform(seed, 200 + n, (I, rank)))
+            continue
+        if strategy == "random_normal":
+            out.append(synth.normal(seed, 400 + n, (I, rank)))
+            continue
+        Xn = np.moveaxis(X, n, 0).reshape(I, -1)
+        u, s, vt = np.linalg.svd(Xn, full_matrices=False)
+        k = min(rank, u.shape[1], vt.shape[0])
+        for r in range(k):
+            i = int(np.argmax(np.abs(u[:, r])))
+            if u[i, r] < 0:
+                u[:, r] *= -1.0
+                vt[r] *= -1.0
+        F = np.zeros((I, rank))
+        pad = synth.normal(seed, 500 + n, (I, rank - k)) * 0.01 if rank > k else None
+        if strategy == "svd":
+            F[:, :k] = u[:, :k]
+            if pad is not None:
+                F[:, k:] = pad
+        elif strategy == "nnsvd":
+            for r in range(k):
+                up, un = np.maximum(u[:, r], 0), np.maximum(-u[:, r], 0)
+                vp, vn = np.maximum(vt[r], 0), np.maximum(-vt[r], 0)
+                pp = np.linalg.norm(up) * np.linalg.norm(vp)
+                nn = np.linalg.norm(un) * np.linalg.norm(vn)
+                F[:, r] = up * np.sqrt(s[r] * pp) if pp >= nn else un * np.sqrt(s[r] * nn)
+            if pad is not None:
+                F[:, k:] = np.abs(pad)
+        elif strategy == "leverage_score":
+            lev = np.sum(u[:, :k] ** 2, axis=1) / k
+            total = lev.sum()
+            if total > np.finfo(np.float32).eps:
+                lev = lev / total
+            F[:, :k] = u[:, :k] * np.sqrt(s[:k]) * np.sqrt(lev * I)[:, None]
+            if pad is not None:
+                F[:, k:] = pad * lev[:, None]
+        else:
+            raise ValueError(f"unknown strategy {strategy!r}")
+        out.append(F)
+    return out
+
+
 def cp_als_accelerated(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
                        trace=None):
     """Restated ``cp_als_accelerated`` (cp/advanced.rs:51-213) in FP64 from

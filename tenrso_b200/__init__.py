@@ -15,6 +15,7 @@ from .dense import (  # noqa: F401
     cp_als_accelerated_dev,
     default_context,
     gram_inverse,
+    initialize_factors,
     khatri_rao,
     mttkrp,
     mttkrp_all_modes,

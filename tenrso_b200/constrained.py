@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import CpConstraintsC, CpInfo, TenrsoError, check
-from .dense import CpDecomp, _ctx_handle, _f32, _i64, _info_to, _prec, _ptr
+from .dense import CpDecomp, _ctx_handle, _f32, _i64, _info_to, _init_ptr, _prec, _ptr
 
 E_INVALID_RANK = 5
 E_INVALID_TOL = 6
@@ -171,15 +171,7 @@ def cp_als_constrained(tensor, rank: int, max_iters: int, tol: float, init="rand
     shape = _i64(t.shape)
     total = int(sum(n * rank for n in t.shape))
     out = np.zeros(max(total, 1), dtype=np.float32)
-    if isinstance(init, str):
-        if init.lower() != "random":
-            raise ValueError("only InitStrategy::Random or injected factors are supported")
-        init_ptr = None
-    else:
-        flat = np.concatenate([_f32(f).ravel() for f in init])
-        if flat.size != total:
-            raise ValueError("initial factors do not match shape x rank")
-        init_ptr = _ptr(flat)
+    init_ptr, _keep = _init_ptr(t, rank, init, seed, ctx)
     hist = np.zeros(max(max_iters, 1), dtype=np.float64)
     info = CpInfo()
     info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))

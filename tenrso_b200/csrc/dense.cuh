@@ -55,6 +55,7 @@ int launch_reconstruct(tsr_ctx* ctx, const FactorTable& ft, int ndim, int R, con
 void init_adjoint_attributes();
 void init_batched_attributes();
 void init_accel_attributes();
+void init_init_attributes();
 
 // SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform (the
 // library's InitStrategy::Random).

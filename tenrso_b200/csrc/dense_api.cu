@@ -648,6 +648,7 @@ void init_kernel_attributes() {
   init_batched_attributes();
   init_accel_attributes();
   init_hicoo_attributes();
+  init_init_attributes();
   done_mask |= 1ull << dev;
 }
 

@@ -250,25 +250,55 @@ def _info_to(info: CpInfo, hist: np.ndarray):
                            final_fit_change=float(info.final_fit_change))
 
 
+INIT_STRATEGIES = {"random": 0, "random_normal": 1, "randomnormal": 1, "svd": 2, "nnsvd": 3,
+                   "leverage_score": 4, "leveragescore": 4}
+
+
+def initialize_factors(tensor, rank: int, init="random", seed: int = 0,
+                       ctx: Optional[Context] = None) -> List[np.ndarray]:
+    """initialize_factors (cp/helpers.rs:192-377) on the device for an
+    InitStrategy name: random, random_normal, svd, nnsvd, leverage_score."""
+    key = str(init).lower()
+    if key not in INIT_STRATEGIES:
+        raise ValueError(f"unknown InitStrategy {init!r}")
+    t = _f32(tensor)
+    total = int(sum(n * rank for n in t.shape))
+    out = np.zeros(max(total, 1), dtype=np.float32)
+    check(_lib.load().tsr_cp_init_f32(_ctx_handle(ctx), _ptr(t), t.ndim, _ptr(_i64(t.shape)),
+                                      rank, INIT_STRATEGIES[key], seed, _ptr(out)))
+    factors, off = [], 0
+    for n in t.shape:
+        factors.append(out[off:off + n * rank].reshape(n, rank).copy())
+        off += n * rank
+    return factors
+
+
+def _init_ptr(t: np.ndarray, rank: int, init, seed: int, ctx):
+    """(pointer, keep-alive array) of the initial factors: None for Random
+    (drawn inside the C call), else the injected or device-initialised ones."""
+    if isinstance(init, str):
+        if init.lower() == "random":
+            return None, None
+        init = initialize_factors(t, rank, init, seed, ctx)
+    total = int(sum(n * rank for n in t.shape))
+    flat = np.concatenate([_f32(f).ravel() for f in init])
+    if flat.size != total:
+        raise ValueError("initial factors do not match shape x rank")
+    return _ptr(flat), flat
+
+
 def cp_als(tensor, rank: int, max_iters: int, tol: float, init="random",
            time_limit: Optional[float] = None, precision="fp32", seed: int = 0,
            ctx: Optional[Context] = None) -> CpDecomp:
     """CP-ALS with tenrso's loop, validation and convergence rules.
-    init: "random" (U(0,1) from the seeded SplitMix64 stream `seed`) or a list
-    of initial factor matrices (the injected initialisation)."""
+    init: an InitStrategy name ("random": U(0,1) from the seeded SplitMix64
+    stream `seed`; "random_normal", "svd", "nnsvd", "leverage_score") or a
+    list of initial factor matrices (the injected initialisation)."""
     t = _f32(tensor)
     shape = _i64(t.shape)
     total = int(sum(n * rank for n in t.shape))
     out = np.zeros(max(total, 1), dtype=np.float32)
-    if isinstance(init, str):
-        if init.lower() != "random":
-            raise ValueError("only InitStrategy::Random or injected factors are supported")
-        init_ptr = None
-    else:
-        flat = np.concatenate([_f32(f).ravel() for f in init])
-        if flat.size != total:
-            raise ValueError("initial factors do not match shape x rank")
-        init_ptr = _ptr(flat)
+    init_ptr, _keep = _init_ptr(t, rank, init, seed, ctx)
     hist = np.zeros(max(max_iters, 1), dtype=np.float64)
     info = CpInfo()
     info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))
@@ -316,15 +346,7 @@ def cp_als_accelerated(tensor, rank: int, max_iters: int, tol: float, init="rand
     shape = _i64(t.shape)
     total = int(sum(n * rank for n in t.shape))
     out = np.zeros(max(total, 1), dtype=np.float32)
-    if isinstance(init, str):
-        if init.lower() != "random":
-            raise ValueError("only InitStrategy::Random or injected factors are supported")
-        init_ptr = None
-    else:
-        flat = np.concatenate([_f32(f).ravel() for f in init])
-        if flat.size != total:
-            raise ValueError("initial factors do not match shape x rank")
-        init_ptr = _ptr(flat)
+    init_ptr, _keep = _init_ptr(t, rank, init, seed, ctx)
     hist = np.zeros(max(max_iters, 1), dtype=np.float64)
     info = CpInfo()
     info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))
