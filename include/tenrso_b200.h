@@ -256,6 +256,15 @@ int tsr_cp_als_accelerated_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim
                                    const float* d_init, int precision, double time_limit_s,
                                    float* d_out_factors, tsr_cp_info* info);
 
+/* One ALS factor update on device data, the building block of a sharded
+ * sweep: U = M G^-1 for the rows x rank fp32 MTTKRP rows d_M and the FP64
+ * R x R Hadamard d_hadamard (solve_least_squares, cp/helpers.rs:455-495, with
+ * its eps*rank*10 ridge retry), the full FP64 Gram U^T U of the new rows into
+ * d_gram and <M, U> (FP64) into *inner_out. rows may be 0 (d_gram = 0). */
+int tsr_als_solve_dev_f32(tsr_ctx* ctx, const float* d_M, int64_t rows, int64_t rank,
+                          const double* d_hadamard, float* d_U, double* d_gram,
+                          double* inner_out, int* ridge_used);
+
 /* initialize_factors (crates/tenrso-decomp/src/cp/helpers.rs:192-377) for
  * every InitStrategy: out_factors receives the concatenated I_n x rank fp32
  * factors. Random and RandomNormal draw from the library's seeded stream

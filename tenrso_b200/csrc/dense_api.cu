@@ -872,6 +872,71 @@ int tsr_gram_inverse_f64(tsr_ctx* ctx, const double* gram, int64_t rank, int ite
   return TSR_OK;
 }
 
+}  // extern "C"
+
+namespace tsr {
+namespace {
+// out = upper triangle of g mirrored to a full symmetric R x R matrix.
+__global__ void symmetrize_kernel(const double* __restrict__ g, int R, double* __restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < R * R; e += gridDim.x * blockDim.x) {
+    const int i = e / R, j = e % R;
+    out[e] = i <= j ? g[i * R + j] : g[j * R + i];
+  }
+}
+}  // namespace
+}  // namespace tsr
+
+extern "C" {
+
+int tsr_als_solve_dev_f32(tsr_ctx* ctx, const float* d_M, int64_t rows, int64_t rank,
+                          const double* d_hadamard, float* d_U, double* d_gram,
+                          double* inner_out, int* ridge_used) {
+  if (!d_hadamard || !d_gram || (rows > 0 && (!d_M || !d_U)))
+    return fail(TSR_E_INVALID_ARG, "null argument");
+  if (rows < 0) return fail(TSR_E_INVALID_ARG, "negative row count");
+  if (rank < 1 || rank > kMaxRank)
+    return fail(TSR_E_UNSUPPORTED, "rank %lld outside 1..%d", (long long)rank, kMaxRank);
+  TSR_TRY(check_ctx(ctx));
+  const int R = (int)rank;
+  const size_t RR = (size_t)R * R;
+  // a 2-mode ALS state whose Gram_0 is the given Hadamard: the inverse of
+  // mode 1 is then that of the Hadamard itself, and the solve of mode 1
+  // writes U = M G^-1, its Gram (into Gram_1) and <M, U>
+  void *gp, *stp;
+  TSR_TRY(slot_get(ctx, SLOT_GRAMS, sizeof(double) * 5 * RR, &gp));
+  TSR_TRY(slot_get(ctx, SLOT_STATE, 256 + sizeof(double), &stp));
+  AlsBuffers b;
+  b.grams = (double*)gp;
+  b.hadam = b.grams + 2 * RR;
+  b.ginv = b.hadam + 2 * RR;
+  b.state = (AlsState*)stp;
+  b.history = (double*)((char*)stp + 256);
+  TSR_CUDA(cudaMemsetAsync(stp, 0, 256 + sizeof(double), ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(b.grams, d_hadamard, sizeof(double) * RR, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+  TSR_TRY(reset_status(ctx));
+  const float ridge = std::numeric_limits<float>::epsilon() * (float)(R * 10);
+  TSR_TRY(launch_chol(ctx, ctx->stream, b, 2, 1, R, ridge, true, 0.0));
+  if (rows > 0)
+    TSR_TRY(launch_solve(ctx, ctx->stream, b, d_M, 1, rows, R, d_U, b.grams + RR, true, 2, 0.0));
+  symmetrize_kernel<<<(unsigned)ceil_div((int64_t)RR, 256), 256, 0, ctx->stream>>>(b.grams + RR,
+                                                                                  R, d_gram);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  AlsState hs;
+  TSR_CUDA(cudaMemcpyAsync(&hs, b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSR_TRY(check_device_status(ctx));
+  if (ridge_used) *ridge_used = hs.ridge_used;
+  if (inner_out) *inner_out = rows > 0 ? hs.inner : 0.0;
+  if (hs.status & DS_NOT_SPD)
+    return fail(TSR_E_NOT_SPD,
+                "Linear algebra error: Gram matrix is not positive definite (ridge %g also "
+                "failed)",
+                (double)ridge);
+  return TSR_OK;
+}
+
 int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
                        int64_t rank, int max_iters, double tol, const float* d_init,
                        int precision, double time_limit_s, float* d_out_factors,
