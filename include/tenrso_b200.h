@@ -366,6 +366,40 @@ int tsr_mttkrp_hicoo_f32(tsr_ctx* ctx, const tsr_hicoo* h, const float* const* f
 int tsr_mttkrp_hicoo_dev_f32(tsr_ctx* ctx, const tsr_hicoo* h, const float* const* d_factors,
                              int64_t rank, int mode, float* d_out);
 
+/* ---- n-mode products: crates/tenrso-kernels/src/nmode.rs ----------------
+ * nmode_product (nmode.rs:72-131): out = tensor x_mode matrix, matrix rows x
+ * cols (row-major) with cols == shape[mode]; out has shape[mode] replaced by
+ * rows. Errors: "Mode {} out of bounds for tensor with rank {}"
+ * (TSR_E_MODE_OOB), "Matrix columns ({}) must match tensor mode-{} size ({})"
+ * (TSR_E_COLS_MISMATCH). fp32 in, fp32 accumulate (the reference sums in T). */
+int tsr_nmode_product_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                          const float* matrix, int64_t rows, int64_t cols, int mode, float* out);
+int tsr_nmode_product_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int64_t* shape,
+                              const float* d_matrix, int64_t rows, int64_t cols, int mode,
+                              float* d_out);
+/* nmode_products_seq (nmode.rs:241-254) / tucker_operator_ordered
+ * (nmode.rs:517-531): products in the given order; cols[t] equals that
+ * mode's size at step t. out_shape gets the result's shape; out may be NULL
+ * to ask for the shape only. */
+int tsr_nmode_products_seq_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                               int n, const int* modes, const float* const* mats,
+                               const int64_t* rows, const int64_t* cols, float* out,
+                               int64_t* out_shape);
+/* tucker_operator (nmode.rs:442-480): a mode -> matrix map applied in
+ * ascending order of rows / mode size (ties by mode index). */
+int tsr_tucker_operator_f32(tsr_ctx* ctx, const float* tensor, int ndim, const int64_t* shape,
+                            int n, const int* modes, const float* const* mats,
+                            const int64_t* rows, const int64_t* cols, float* out,
+                            int64_t* out_shape);
+/* tucker_reconstruct (nmode.rs:576-611): core x_0 U_0 ... x_{N-1} U_{N-1};
+ * "Number of factor matrices ({}) must match core rank ({})" (TSR_E_NFACTORS),
+ * "Factor matrix {} has {} columns, expected {} (core mode-{} size)"
+ * (TSR_E_RANK_MISMATCH). */
+int tsr_tucker_reconstruct_f32(tsr_ctx* ctx, const float* core, int ndim,
+                               const int64_t* core_shape, int n_factors,
+                               const float* const* factors, const int64_t* rows,
+                               const int64_t* cols, float* out, int64_t* out_shape);
+
 /* ---- CP reconstruction and its adjoint ----------------------------------
  * tenrso_kernels::cp_reconstruct (crates/tenrso-kernels/src/outer.rs:223-274):
  * out (row-major, prod of factor_rows) = sum_r w_r U_0[:,r] o ... o U_{N-1}[:,r].

@@ -246,6 +246,19 @@ def csf_from_coo(idx: np.ndarray, vals: np.ndarray, mode_order):
     return fp, fi, vout[:nv].copy()
 
 
+def nmode_product(X: np.ndarray, M: np.ndarray, mode: int) -> np.ndarray:
+    """Restated ``nmode_product`` (nmode.rs:72-131) in FP64: unfold along
+    `mode`, M . X_(mode), fold back with shape[mode] replaced by M's rows."""
+    X = np.asarray(X, dtype=np.float64)
+    M = np.asarray(M, dtype=np.float64)
+    if not 0 <= mode < X.ndim:
+        raise ValueError(f"Mode {mode} out of bounds for tensor with rank {X.ndim}")
+    if M.shape[1] != X.shape[mode]:
+        raise ValueError(f"Matrix columns ({M.shape[1]}) must match tensor mode-{mode} size "
+                         f"({X.shape[mode]})")
+    return np.moveaxis(np.tensordot(M, X, axes=(1, mode)), 0, mode)
+
+
 def hicoo_from_coo(idx, vals, block_shape):
     """Restated ``HiCooTensor::from_coo`` (hicoo.rs:118-203): block
     coordinates i // b and local coordinates i % b, a stable sort by block

@@ -68,3 +68,11 @@ from .adjoint import (  # noqa: F401
 from .batched import BatchedCpAls  # noqa: F401
 
 __version__ = "0.1.0"
+
+from .tucker import (  # noqa: F401
+    nmode_product,
+    nmode_products_seq,
+    tucker_operator,
+    tucker_operator_ordered,
+    tucker_reconstruct,
+)

@@ -87,6 +87,11 @@ SIGNATURES = {
     "tsr_mttkrp_hicoo_dev_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
     "tsr_als_solve_dev_f32": (C.c_int, [P, P, I64, I64, P, P, P, C.POINTER(C.c_double),
                                         C.POINTER(C.c_int)]),
+    "tsr_nmode_product_f32": (C.c_int, [P, P, C.c_int, P, P, I64, I64, C.c_int, P]),
+    "tsr_nmode_product_dev_f32": (C.c_int, [P, P, C.c_int, P, P, I64, I64, C.c_int, P]),
+    "tsr_nmode_products_seq_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P, P]),
+    "tsr_tucker_operator_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P, P]),
+    "tsr_tucker_reconstruct_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P]),
     "tsr_cp_init_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_uint64, P]),
     "tsr_cp_init_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_uint64, P]),
     "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),
