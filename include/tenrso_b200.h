@@ -215,14 +215,23 @@ int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
  *   validate_nonneg_input: with nonnegative, a tensor holding a negative
  *       entry is rejected with TSR_E_NONNEG_VIOLATION (core.rs:265-267,
  *       helpers.rs:705-716).
- * l2 or l1 negative or not finite gives TSR_E_INVALID_REGULARIZATION.
- * Orthogonality (QR after each update) and Tikhonov of order > 0 are not
- * applied by the GPU sweep; the host layer rejects them. */
+ *   orthogonal: each new factor (after the threshold and the projection)
+ *       replaced by the Q of its QR factorization (core.rs:361-364,
+ *       helpers.rs:582-607), taken with a positive diagonal in R (Cholesky of
+ *       U^T U in FP64); linearly dependent columns give TSR_E_NOT_SPD;
+ *   tikhonov_order > 0: tikhonov_lambda times apply_tikhonov_to_gram's
+ *       finite-difference penalty added to the Gram instead of l2
+ *       (core.rs:327-344).
+ * l2, l1 or tikhonov_lambda negative or not finite gives
+ * TSR_E_INVALID_REGULARIZATION. */
 typedef struct tsr_cp_constraints {
   double l2;
   double l1;
   int nonnegative;
   int validate_nonneg_input;
+  int orthogonal;         /* QR-orthonormalize each updated factor (core.rs:361-364) */
+  int tikhonov_order;     /* > 0: RegularizationType::Tikhonov{lambda, order}'s */
+  double tikhonov_lambda; /*   finite-difference penalty (helpers.rs:630-700) */
 } tsr_cp_constraints;
 
 /* cp_als_constrained (core.rs:225-400) on the dense path; arguments as

@@ -158,16 +158,55 @@ def cp_als(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
     return out, info
 
 
+def tikhonov_penalty(n: int, order: int) -> np.ndarray:
+    """The matrix apply_tikhonov_to_gram (cp/helpers.rs:630-700) adds, per
+    unit lambda: order 0 I; order 1 D1^T D1 (nothing for n < 2); order >= 2
+    the reference's banded form with diagonal 1, 5, 6.., 5, 1, first
+    off-diagonal -2, -4.., -4, -2, second off-diagonal 1 (I for n < 3)."""
+    P = np.zeros((n, n))
+    if order == 0:
+        return np.eye(n)
+    if order == 1:
+        if n >= 2:
+            for i in range(n):
+                P[i, i] = 1.0 if i in (0, n - 1) else 2.0
+                if i + 1 < n:
+                    P[i, i + 1] = P[i + 1, i] = -1.0
+        return P
+    if n < 3:
+        return np.eye(n)
+    for i in range(n):
+        P[i, i] = 1.0 if i in (0, n - 1) else (5.0 if i in (1, n - 2) else 6.0)
+        if i + 1 < n:
+            P[i, i + 1] = P[i + 1, i] = -2.0 if i in (0, n - 2) else -4.0
+        if i + 2 < n:
+            P[i, i + 2] = P[i + 2, i] = 1.0
+    return P
+
+
+def orthonormalize(F: np.ndarray) -> np.ndarray:
+    """orthonormalize_factor (cp/helpers.rs:582-607): the thin Q of a QR
+    factorization. scirs2-linalg's QR leaves the signs to its algorithm; Q is
+    taken here with a positive diagonal in R (the unique such QR)."""
+    q, r = np.linalg.qr(F)
+    d = np.sign(np.diag(r))
+    d[d == 0] = 1.0
+    return q * d[None, :]
+
+
 def cp_als_constrained(X: np.ndarray, rank: int, max_iters: int, tol: float, init_factors,
-                       l2: float = 0.0, l1: float = 0.0, nonneg: bool = False):
+                       l2: float = 0.0, l1: float = 0.0, nonneg: bool = False,
+                       orthogonal: bool = False, tikhonov=None):
     """Restated ``cp_als_constrained`` (cp/core.rs:225-400) in FP64 from
     injected factors, for small tensors: per mode MTTKRP (the restated C
     kernel), Hadamard of the other Grams, ridge l2 on its diagonal
     (core.rs:336-343), the restated solve, soft threshold by l1
-    (helpers.rs:610-623), projection onto >= 0 (core.rs:356-359); the fit and
-    stopping rules of core.rs:366-392 (the same as cp_als). The input
-    non-negativity check and the initial projection (core.rs:265-276) are
-    applied too. Returns (factors, info dict)."""
+    (helpers.rs:610-623), projection onto >= 0 (core.rs:356-359), the QR
+    orthonormalization (core.rs:361-364); tikhonov = (lambda, order) with
+    order > 0 replaces the ridge by lambda * tikhonov_penalty (core.rs:327-334);
+    the fit and stopping rules of core.rs:366-392 (the same as cp_als). The
+    input non-negativity check and the initial projection (core.rs:265-276)
+    are applied too. Returns (factors, info dict)."""
     X = np.ascontiguousarray(X, dtype=np.float64)
     if nonneg and (X < 0).any():
         raise ValueError("Non-negative constraint violated: input tensor contains negative values")
@@ -185,13 +224,17 @@ def cp_als_constrained(X: np.ndarray, rank: int, max_iters: int, tol: float, ini
             for m in range(X.ndim):
                 if m != n:
                     G *= gram(U[m])
-            if l2 > 0.0:
+            if tikhonov is not None and tikhonov[1] > 0:
+                G += tikhonov[0] * tikhonov_penalty(rank, tikhonov[1])
+            elif l2 > 0.0:
                 G[np.diag_indices(rank)] += l2
             U[n] = solve(M, G)
             if l1 > 0.0:
                 U[n] = np.where(U[n] > l1, U[n] - l1, np.where(U[n] < -l1, U[n] + l1, 0.0))
             if nonneg:
                 U[n] = np.maximum(U[n], 0.0)
+            if orthogonal:
+                U[n] = orthonormalize(U[n])
         # compute_fit (helpers.rs:513-579)
         inner = float(np.sum(mttkrp(X, U, 0) * U[0]))
         H = np.ones((rank, rank))

@@ -24,6 +24,9 @@ class CpConstraintsC(C.Structure):
         ("l1", C.c_double),
         ("nonnegative", C.c_int),
         ("validate_nonneg_input", C.c_int),
+        ("orthogonal", C.c_int),
+        ("tikhonov_order", C.c_int),
+        ("tikhonov_lambda", C.c_double),
     ]
 
 

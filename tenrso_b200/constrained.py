@@ -1,5 +1,6 @@
-"""cp_als_constrained over the C ABI: the dense CP-ALS sweep with a ridge on
-the Gram diagonal, soft-thresholding and non-negativity applied on the GPU.
+"""cp_als_constrained over the C ABI: the dense CP-ALS sweep with a ridge (or
+a Tikhonov finite-difference penalty) on the Gram, soft-thresholding,
+non-negativity and orthonormalization applied on the GPU.
 
   RegularizationType (validate, l1/l2 components)  crates/tenrso-decomp/src/cp/types.rs:65-192
   CpConstraints (+ constructors, effective_l1/l2)   crates/tenrso-decomp/src/cp/types.rs:199-309
@@ -7,8 +8,8 @@ the Gram diagonal, soft-thresholding and non-negativity applied on the GPU.
 
 The checks run in tenrso's order and raise its messages (as `TenrsoError`
 with the C status of the matching `CpError`) before anything reaches the GPU.
-Orthogonality (a QR after every update) and Tikhonov regularization of order
-> 0 are not part of the GPU sweep and are rejected with TSR_E_UNSUPPORTED.
+Orthogonality (a QR after every update, taken with a positive diagonal in R)
+and Tikhonov regularization of any order run inside the GPU sweep.
 """
 from __future__ import annotations
 
@@ -24,7 +25,6 @@ from .dense import CpDecomp, _ctx_handle, _f32, _i64, _info_to, _init_ptr, _prec
 
 E_INVALID_RANK = 5
 E_INVALID_TOL = 6
-E_UNSUPPORTED = 14
 E_INVALID_REGULARIZATION = 19
 
 
@@ -150,13 +150,12 @@ def _validate(shape, rank: int, tol: float, c: CpConstraints) -> CpConstraintsC:
     c.regularization.validate()
     if c.regularization.kind == "none" and c.l2_reg < 0.0:
         raise TenrsoError(E_INVALID_TOL, f"Invalid tolerance: {_disp(c.l2_reg)}")
-    if c.orthogonal:
-        raise TenrsoError(E_UNSUPPORTED, "orthogonal constraints are not applied by the GPU sweep")
-    if c.regularization.kind == "tikhonov" and c.regularization.order > 0:
-        raise TenrsoError(E_UNSUPPORTED,
-                          "Tikhonov regularization of order > 0 is not applied by the GPU sweep")
+    reg = c.regularization
+    tik = reg.kind == "tikhonov" and reg.order > 0
     return CpConstraintsC(float(c.effective_l2()), float(c.effective_l1()),
-                          1 if c.nonnegative else 0, 1 if c.validate_nonneg_input else 0)
+                          1 if c.nonnegative else 0, 1 if c.validate_nonneg_input else 0,
+                          1 if c.orthogonal else 0, int(reg.order) if tik else 0,
+                          float(reg.lam) if tik else 0.0)
 
 
 def cp_als_constrained(tensor, rank: int, max_iters: int, tol: float, init="random",

@@ -381,6 +381,40 @@ __device__ __forceinline__ void add_diagonal(double (&a)[RB][GjLayout<RB>::CB], 
       if (ty + 16 * ai == tx + kGjCW * bj && ty + 16 * ai < R) a[ai][bj] += l2;
 }
 
+// Coefficient (i, j) of the finite-difference penalty that
+// apply_tikhonov_to_gram (helpers.rs:630-700) adds, times lambda, to an
+// n x n Gram: order 1 D1^T D1 (n >= 2; nothing for n < 2), order >= 2 the
+// reference's banded second-order form (n >= 3; lambda I for n < 3).
+__device__ __forceinline__ double tikhonov_coef(int i, int j, int n, int order) {
+  if (order == 1) {
+    if (n < 2) return 0.0;
+    if (i == j) return (i == 0 || i == n - 1) ? 1.0 : 2.0;
+    return (i - j == 1 || j - i == 1) ? -1.0 : 0.0;
+  }
+  if (n < 3) return i == j ? 1.0 : 0.0;
+  if (i == j) return (i == 0 || i == n - 1) ? 1.0 : ((i == 1 || i == n - 2) ? 5.0 : 6.0);
+  const int lo = i < j ? i : j, d = i < j ? j - i : i - j;
+  if (d == 1) return (lo == 0 || lo == n - 2) ? -2.0 : -4.0;
+  if (d == 2) return 1.0;
+  return 0.0;
+}
+
+// a += lambda * P (the Tikhonov penalty of order > 0) on this bulk thread's
+// entries.
+template <int RB>
+__device__ __forceinline__ void add_tikhonov(double (&a)[RB][GjLayout<RB>::CB], int R,
+                                             double lambda, int order) {
+  constexpr int CB = GjLayout<RB>::CB;
+  const int t = gj_bulk_index(), ty = t / kGjCW, tx = t % kGjCW;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < CB; ++bj) {
+      const int i = ty + 16 * ai, j = tx + kGjCW * bj;
+      if (i < R && j < R) a[ai][bj] += lambda * tikhonov_coef(i, j, R, order);
+    }
+}
+
 // fit, fit_history, oscillation and convergence rules (helpers.rs:513-530,
 // core.rs:142-166) of the sweep whose last solve has finished, from the
 // scalars that solve accumulated: ||X||^2 + ||Xhat||^2 - 2 <X, Xhat>. Called
@@ -446,7 +480,8 @@ __global__ void fit_kernel(AlsBuffers b, double tol) {
 template <int RB>
 __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int ndim, int mode, int R,
                                                    float ridge_eps, int last, double tol,
-                                                   double l2, TraceSlot tr) {
+                                                   double l2, int tik_order, double tik_lambda,
+                                                   TraceSlot tr) {
   __shared__ GjShared<RB> gsh;
   trace_begin(tr);
   AlsState* st = b.state;
@@ -465,6 +500,7 @@ __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int n
   if (bulk) {
     load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, 0.0, a, true);
     if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+    if (tik_order > 0) add_tikhonov<RB>(a, R, tik_lambda, tik_order);
   }
   // solve_least_squares solves gram^T x = b (helpers.rs:462,471); G is
   // symmetric by construction so G^T = G.
@@ -474,6 +510,7 @@ __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int n
     if (bulk) {
       load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R, (double)ridge_eps, a, false);
       if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+      if (tik_order > 0) add_tikhonov<RB>(a, R, tik_lambda, tik_order);
     }
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 1;
@@ -497,6 +534,7 @@ __global__ void __launch_bounds__(kGjThreads, 1) chol_kernel(AlsBuffers b, int n
       load_hadamard<RB>(b.grams, b.hadam, ndim, mode, R,
                         (double)ridge_eps * fmax(gsh.scale, 1.0), a, false);
       if (l2 != 0.0) add_diagonal<RB>(a, R, l2);
+      if (tik_order > 0) add_tikhonov<RB>(a, R, tik_lambda, tik_order);
     }
     ok = gj_inverse<RB>(a, gsh);
     if (threadIdx.x == 0) st->ridge_used = 2;
@@ -788,9 +826,197 @@ solve_kernel(AlsBuffers b, const float* __restrict__ partials, int splits, int64
   trace_end(tr);
 }
 
+// orthonormalize_factor, step 1 (one CTA): the Cholesky factor R of the
+// factor's Gram (upper triangle in gram, from the solve), R^-1 into b.ginv;
+// gram (and, for the last mode, <X, Xhat> and ||Xhat||^2) zeroed for step 2.
+__global__ void __launch_bounds__(256) orth_chol_kernel(AlsBuffers b, int R, double* gram,
+                                                        int last) {
+  extern __shared__ __align__(16) double oa[];  // R x R working copy
+  __shared__ int bad;
+  AlsState* st = b.state;
+  if (st->done) return;
+  if (threadIdx.x == 0) bad = 0;
+  for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+    const int i = e / R, j = e % R;
+    oa[e] = i <= j ? gram[i * R + j] : 0.0;
+  }
+  __syncthreads();
+  // right-looking Cholesky on the upper triangle: row k of R, then the
+  // trailing update
+  for (int k = 0; k < R; ++k) {
+    if (threadIdx.x == 0) {
+      const double d = oa[k * R + k];
+      if (!(d > 0.0) || !isfinite(d)) bad = 1;
+      oa[k * R + k] = sqrt(fmax(d, 0.0));
+    }
+    __syncthreads();
+    if (bad) break;
+    const double dk = oa[k * R + k];
+    for (int j = k + 1 + threadIdx.x; j < R; j += blockDim.x) oa[k * R + j] /= dk;
+    __syncthreads();
+    const int m = R - k - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = k + 1 + e / m, j = k + 1 + e % m;
+      if (i <= j) oa[i * R + j] -= oa[k * R + i] * oa[k * R + j];
+    }
+    __syncthreads();
+  }
+  if (bad) {
+    if (threadIdx.x == 0) {
+      st->status |= DS_NOT_SPD;
+      st->done = 1;
+    }
+    return;
+  }
+  // R^-1 (upper triangular), one column per thread by back substitution
+  for (int j = threadIdx.x; j < R; j += blockDim.x) {
+    double* x = b.ginv + j;  // column j, stride R
+    for (int i = j + 1; i < R; ++i) x[i * R] = 0.0;
+    x[j * R] = 1.0 / oa[j * R + j];
+    for (int i = j - 1; i >= 0; --i) {
+      double t = 0.0;
+      for (int l = i + 1; l <= j; ++l) t += oa[i * R + l] * x[l * R];
+      x[i * R] = -t / oa[i * R + i];
+    }
+  }
+  for (int e = threadIdx.x; e < R * R; e += blockDim.x) gram[e] = 0.0;
+  if (last && threadIdx.x == 0) {
+    st->inner = 0.0;
+    st->xhat_sq = 0.0;
+  }
+}
+
+// orthonormalize_factor, step 2: Q = U R^-1 row by row (FP64, stored fp32),
+// Q^T Q into gram (upper triangle, FP64 atomics) and, for the last mode,
+// <M, Q> (M = the sum of the split partials) and ||Xhat||^2 = sum(H o Q^T Q).
+template <int RB>
+__global__ void __launch_bounds__(256)
+orth_apply_kernel(AlsBuffers b, int ndim, int R, int64_t rows, float* __restrict__ U,
+                  double* __restrict__ gram, int last, const float* __restrict__ partials,
+                  int splits) {
+  extern __shared__ __align__(16) double os[];
+  __shared__ double red[16];
+  AlsState* st = b.state;
+  if (st->done) return;
+  constexpr int rpc = 16;
+  double* Ri = os;            // R x R
+  double* Qs = os + R * R;    // rpc x R
+  for (int e = threadIdx.x; e < R * R; e += blockDim.x) Ri[e] = b.ginv[e];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[RB][RB];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = 0.0;
+  double ip = 0.0;
+  const int64_t pstride = rows * R;
+  for (int64_t r0 = (int64_t)blockIdx.x * rpc; r0 < rows; r0 += (int64_t)gridDim.x * rpc) {
+    const int nr = (int)(rows - r0 < rpc ? rows - r0 : rpc);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
+      const int i = e / R, c = e % R;
+      const float* u = U + (r0 + i) * R;
+      double q = 0.0;
+      for (int k = 0; k <= c; ++k) q = fma((double)u[k], Ri[k * R + c], q);
+      Qs[e] = q;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * R; e += blockDim.x) {
+      const float qf = (float)Qs[e];
+      const int64_t g = r0 * R + e;
+      U[g] = qf;
+      Qs[e] = (double)qf;  // the stored value enters the Gram and the fit
+      if (last) {
+        double m = 0.0;
+        for (int p = 0; p < splits; ++p) m += (double)partials[(int64_t)p * pstride + g];
+        ip += m * (double)qf;
+      }
+    }
+    __syncthreads();
+    for (int i = 0; i < nr; ++i) {
+      double x[RB], y[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) x[ai] = ty + 16 * ai < R ? Qs[i * R + ty + 16 * ai] : 0.0;
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) y[bj] = tx + 16 * bj < R ? Qs[i * R + tx + 16 * bj] : 0.0;
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = fma(x[ai], y[bj], acc[ai][bj]);
+    }
+  }
+  double xs = 0.0;
+  const double* H = b.hadam + (int64_t)(ndim - 1) * R * R;
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int a = ty + 16 * ai, c = tx + 16 * bj;
+      if (a < R && c < R && c >= a) {
+        atomicAdd(gram + a * R + c, acc[ai][bj]);
+        if (last) xs += (c == a ? 1.0 : 2.0) * __ldg(H + a * R + c) * acc[ai][bj];
+      }
+    }
+  if (!last) return;
+  for (int o = 16; o > 0; o >>= 1) {
+    ip += __shfl_down_sync(0xffffffffu, ip, o);
+    xs += __shfl_down_sync(0xffffffffu, xs, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = ip;
+    red[8 + (threadIdx.x >> 5)] = xs;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, x = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += red[w];
+      x += red[8 + w];
+    }
+    atomicAdd(&st->inner, a);
+    atomicAdd(&st->xhat_sq, x);
+  }
+}
+
 }  // namespace
 
+int launch_orthonormalize(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode,
+                          int R, int64_t rows, float* U, double* gram, bool last,
+                          const float* partials, int splits) {
+  (void)mode;
+  if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
+  orth_chol_kernel<<<1, 256, sizeof(double) * R * R, s>>>(b, R, gram, last ? 1 : 0);
+  const unsigned grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(rows, 16), 2 * (int64_t)ctx->sm_count));
+  const size_t smem = sizeof(double) * ((size_t)R * R + 16 * (size_t)R);
+#define TSR_ORTH(RB)                                                                  \
+  orth_apply_kernel<RB><<<grid, 256, smem, s>>>(b, ndim, R, rows, U, gram, last ? 1 : 0, \
+                                                partials, splits)
+  switch ((R + 15) / 16) {
+    case 1: TSR_ORTH(1); break;
+    case 2: TSR_ORTH(2); break;
+    case 3: TSR_ORTH(3); break;
+    case 4: TSR_ORTH(4); break;
+    case 5: TSR_ORTH(5); break;
+    case 6: TSR_ORTH(6); break;
+    default: TSR_ORTH(7); break;
+  }
+#undef TSR_ORTH
+  ctx->launches += 2;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
 void init_als_attributes() {
+  cudaFuncSetAttribute(orth_chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(double) * kMaxRank * kMaxRank));
+  cudaFuncSetAttribute(orth_apply_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(orth_apply_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(solve_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(solve_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(solve_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -831,18 +1057,23 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 }
 
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last, double tol, double l2) {
+                float ridge_eps, bool last, double tol, double l2, int tik_order,
+                double tik_lambda) {
   if (R > kMaxRank) return fail(TSR_E_UNSUPPORTED, "rank %d too large for the FP64 solve", R);
   const TraceSlot tr = trace_slot(ctx, TRACE_INVERSE, mode);
   const int lst = last ? 1 : 0;
   switch ((R + 15) / 16) {
-    case 1: chol_kernel<1><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    case 2: chol_kernel<2><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    case 3: chol_kernel<3><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    case 4: chol_kernel<4><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    case 5: chol_kernel<5><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    case 6: chol_kernel<6><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
-    default: chol_kernel<7><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tr); break;
+#define TSR_CHOL(RB)                                                                       \
+  chol_kernel<RB><<<1, kGjThreads, 0, s>>>(b, ndim, mode, R, ridge_eps, lst, tol, l2, tik_order, \
+                                           tik_lambda, tr)
+    case 1: TSR_CHOL(1); break;
+    case 2: TSR_CHOL(2); break;
+    case 3: TSR_CHOL(3); break;
+    case 4: TSR_CHOL(4); break;
+    case 5: TSR_CHOL(5); break;
+    case 6: TSR_CHOL(6); break;
+    default: TSR_CHOL(7); break;
+#undef TSR_CHOL
   }
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());

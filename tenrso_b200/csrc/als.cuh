@@ -74,8 +74,20 @@ int launch_norm_sq(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, doub
 // l2 >= 0 is added to the Hadamard's diagonal before the inverse (the ridge of
 // cp_als_constrained, core.rs:336-343); the stored Hadamard (used by the fit)
 // stays unshifted.
+// tik_order > 0 adds tik_lambda times the finite-difference penalty of
+// apply_tikhonov_to_gram (helpers.rs:630-700) instead.
 int launch_chol(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode, int R,
-                float ridge_eps, bool last, double tol, double l2 = 0.0);
+                float ridge_eps, bool last, double tol, double l2 = 0.0, int tik_order = 0,
+                double tik_lambda = 0.0);
+// orthonormalize_factor (helpers.rs:582-607) after this mode's solve: the
+// factor U (rows x R, in place) becomes Q = U R^-1 with U^T U = R^T R
+// (Cholesky in FP64 of the Gram the solve accumulated; Q's R has a positive
+// diagonal), gram is recomputed as Q^T Q and, for the last mode, <M, Q> and
+// ||Xhat||^2 are re-formed from the split partials. A Gram that is not
+// positive definite (linearly dependent columns) stops the run with DS_NOT_SPD.
+int launch_orthonormalize(tsr_ctx* ctx, cudaStream_t s, const AlsBuffers& b, int ndim, int mode,
+                          int R, int64_t rows, float* U, double* gram, bool last,
+                          const float* partials, int splits);
 // Clamp n floats at zero (non-negative initial factors, core.rs:271-276).
 int launch_clamp_nonneg(tsr_ctx* ctx, cudaStream_t s, float* U, int64_t n);
 // Sets *flag to 1 if any of the n values is negative (helpers.rs:705-716).

@@ -278,6 +278,9 @@ struct SweepArgs {
   double l2;   // cp_als_constrained: Gram ridge, soft threshold, projection
   float l1;
   int nonneg;
+  int orth;           // orthonormalize each updated factor (QR)
+  int tik_order;      // Tikhonov penalty of order > 0 on the Gram
+  double tik_lambda;
   FactorTable ft;
   const void* op_ptrs[3 * kMaxModes];
   float* partials;
@@ -295,7 +298,8 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
   TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[0], 0));
   for (int n = 0; n < a.ndim; ++n) {
     const bool last = n == a.ndim - 1;
-    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last, a.tol, a.l2));
+    TSR_TRY(launch_chol(ctx, B, a.b, a.ndim, n, a.R, a.ridge, last, a.tol, a.l2, a.tik_order,
+                        a.tik_lambda));
     TSR_CUDA(cudaEventRecord(ctx->ev[1 + 2 * n], B));
     float* partials = a.partials;
     int splits = 1;
@@ -314,6 +318,10 @@ static int enqueue_sweep(tsr_ctx* ctx, const SweepArgs& a, const std::vector<Mod
     TSR_TRY(launch_solve(ctx, A, a.b, partials, splits, a.shape[n], a.R,
                          const_cast<float*>(a.ft.ptr[n]), a.b.grams + (size_t)n * a.R * a.R,
                          last, a.ndim, a.tol, a.l1, a.nonneg, img, a.d3.n_pad));
+    if (a.orth)  // core.rs:361-364, after the soft threshold and the projection
+      TSR_TRY(launch_orthonormalize(ctx, A, a.b, a.ndim, n, a.R, a.shape[n],
+                                    const_cast<float*>(a.ft.ptr[n]),
+                                    a.b.grams + (size_t)n * a.R * a.R, last, partials, splits));
     if (!last) {  // the next inverse needs this mode's Gram
       TSR_CUDA(cudaEventRecord(ctx->ev[2 + 2 * n], A));
       TSR_CUDA(cudaStreamWaitEvent(B, ctx->ev[2 + 2 * n], 0));
@@ -348,6 +356,13 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     if (!(cons->l1 >= 0.0) || !std::isfinite(cons->l1))
       return fail(TSR_E_INVALID_REGULARIZATION,
                   "Invalid regularization parameter: L1 lambda must be >= 0, got %g", cons->l1);
+    if (cons->tikhonov_order < 0)
+      return fail(TSR_E_INVALID_ARG, "negative Tikhonov order %d", cons->tikhonov_order);
+    if (cons->tikhonov_order > 0 &&
+        (!(cons->tikhonov_lambda >= 0.0) || !std::isfinite(cons->tikhonov_lambda)))
+      return fail(TSR_E_INVALID_REGULARIZATION,
+                  "Invalid regularization parameter: Tikhonov lambda must be >= 0, got %g",
+                  cons->tikhonov_lambda);
   }
   const int R = (int)rank;
   const int64_t n = numel(ndim, shape);
@@ -367,6 +382,12 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     a.l2 = cons->l2;
     a.l1 = (float)cons->l1;  // the threshold in the factors' type (core.rs:351)
     a.nonneg = cons->nonnegative ? 1 : 0;
+    a.orth = cons->orthogonal ? 1 : 0;
+    if (cons->tikhonov_order > 0) {  // core.rs:330-334: replaces the ridge
+      a.tik_order = cons->tikhonov_order;
+      a.tik_lambda = cons->tikhonov_lambda;
+      a.l2 = 0.0;
+    }
   }
 
   // factors live in d_out for the whole run (updated in place)
@@ -421,8 +442,11 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
   std::vector<ModeOperand> ops(ndim);
   size_t pmax = 0;
   // 3-way BF16x3: one bf16 hi/lo copy of X read by every mode (no unfoldings)
+  // (the orthonormalisation rewrites a factor after its solve, so the solve's
+  // B image would be stale: that run takes the per-mode unfoldings)
   const bool d3 = !sp && max_iters > 0 && precision == TSR_PREC_BF16X3 &&
-                  dense3_supported(ndim, shape, R) && ((uintptr_t)dX & 15) == 0;
+                  dense3_supported(ndim, shape, R) && ((uintptr_t)dX & 15) == 0 &&
+                  !(cons && cons->orthogonal);
   const bool fused_unfold = !d3 && !sp && max_iters > 0 && unfold3_supported(ndim, shape);
   if (d3) {
     Dense3& d = a.d3;

@@ -35,13 +35,26 @@ def test_regularization_components_and_validation():
     (5, 0.0, CC(), 5, "Invalid rank: 5"),
     (2, 1.0, CC(), 6, "Invalid tolerance: 1"),
     (2, 0.0, CC(l2_reg=-0.5), 6, "Invalid tolerance: -0.5"),
-    (2, 0.0, CC.orthogonal_only(), 14, "orthogonal"),
-    (2, 0.0, CC.tikhonov(0.1, 2), 14, "Tikhonov"),
 ])
 def test_validation_order_without_device(rank, tol, c, status, msg):
     with pytest.raises(tb.TenrsoError, match=msg) as e:
         tb.cp_als_constrained(np.ones((4, 4, 4)), rank, 3, tol, constraints=c)
     assert e.value.status == status
+
+
+def test_oracle_tikhonov_penalty_and_qr(orc):
+    """apply_tikhonov_to_gram (helpers.rs:630-700) as matrices, and the
+    orthonormalization's sign convention."""
+    assert not orc.tikhonov_penalty(1, 1).any()
+    D1 = np.diff(np.eye(4), axis=0)
+    assert np.array_equal(orc.tikhonov_penalty(4, 1), D1.T @ D1)
+    P = orc.tikhonov_penalty(6, 2)
+    assert np.diag(P).tolist() == [1, 5, 6, 6, 5, 1]
+    assert np.diag(P, 1).tolist() == [-2, -4, -4, -4, -2] and np.diag(P, 2).tolist() == [1] * 4
+    assert np.array_equal(orc.tikhonov_penalty(2, 2), np.eye(2))
+    F = np.random.default_rng(0).standard_normal((9, 3))
+    Q = orc.orthonormalize(F)
+    assert np.allclose(Q.T @ Q, np.eye(3)) and np.all(np.diag(Q.T @ F) > 0)
 
 
 def test_oracle_without_constraints_is_cp_als(orc):
@@ -66,6 +79,10 @@ def _case(shape, rank, seed, dist):
     ("l2", CC.l2_regularized(0.5), dict(l2=0.5)),
     ("elastic", CC.elastic_net(0.02, 0.5), dict(l2=0.01, l1=0.01)),
     ("nonneg+l2", CC(nonnegative=True, l2_reg=0.25), dict(l2=0.25, nonneg=True)),
+    ("orthogonal", CC.orthogonal_only(), dict(orthogonal=True)),
+    ("orthogonal+l2", CC(orthogonal=True, l2_reg=0.1), dict(orthogonal=True, l2=0.1)),
+    ("tikhonov1", CC.tikhonov(0.3, 1), dict(tikhonov=(0.3, 1))),
+    ("tikhonov2", CC.tikhonov(0.05, 2), dict(tikhonov=(0.05, 2))),
 ])
 def test_constrained_fit_vs_oracle(orc, precision, name, c, kw):
     X, init = _case((48, 40, 36), 6, 0xC2, "uniform")
@@ -78,6 +95,26 @@ def test_constrained_fit_vs_oracle(orc, precision, name, c, kw):
         assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 2e-3, name
     if kw.get("nonneg"):
         assert all((f >= 0).all() for f in res.factors)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("R,order", [(1, 1), (2, 2), (3, 2)])
+def test_tikhonov_small_rank_rules(orc, R, order):
+    """Order 1 adds nothing at rank 1; order 2 falls back to the ridge below
+    rank 3 (helpers.rs:649, 695-699)."""
+    X, init = _case((12, 10, 9), R, 11, "uniform")
+    res = tb.cp_als_constrained(X, R, 6, 0.0, init=init, constraints=CC.tikhonov(0.2, order))
+    _, info = orc.cp_als_constrained(X, R, 6, 0.0, [f.astype(np.float64) for f in init],
+                                     tikhonov=(0.2, order))
+    assert np.allclose(res.convergence.fit_history, info["fit_history"], atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_orthogonal_factors_are_orthonormal():
+    X, init = _case((30, 25, 20), 4, 13, "normal")
+    res = tb.cp_als_constrained(X, 4, 5, 0.0, init=init, constraints=CC.orthogonal_only())
+    for f in res.factors:
+        assert np.allclose(f.T @ f, np.eye(4), atol=1e-5)
 
 
 @pytest.mark.gpu
