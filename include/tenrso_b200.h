@@ -204,6 +204,18 @@ int tsr_cp_als_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, const int6
                        int precision, double time_limit_s, float* d_out_factors,
                        tsr_cp_info* info);
 
+/* The f64 instantiation of the drop-in: mttkrp<f64> (mttkrp.rs:74-146) and
+ * cp_als<f64> (cp/core.rs:59-182) with FP64 tensor, factors, MTTKRP, Gram,
+ * solve and fit (host buffers; the tensor row-major). Arguments, validation
+ * and messages as tsr_mttkrp_f32 / tsr_cp_als_f32; init_factors NULL draws
+ * InitStrategy::Random from the library's seeded stream `seed` in FP64. */
+int tsr_mttkrp_f64(tsr_ctx* ctx, const double* tensor, int ndim, const int64_t* shape,
+                   const double* const* factors, int n_factors, const int64_t* factor_rows,
+                   const int64_t* factor_cols, int mode, double* out);
+int tsr_cp_als_f64(tsr_ctx* ctx, const double* tensor, int ndim, const int64_t* shape,
+                   int64_t rank, int max_iters, double tol, const double* init_factors,
+                   uint64_t seed, double time_limit_s, double* out_factors, tsr_cp_info* info);
+
 /* Constraints of cp_als_constrained (crates/tenrso-decomp/src/cp/types.rs:199-225,
  * core.rs:225-400) in the form the sweep applies them:
  *   l2  effective_l2() (types.rs:298-303): added to the diagonal of the Gram

@@ -11,6 +11,8 @@ from .dense import (  # noqa: F401
     CpDecomp,
     cp_als,
     cp_als_dev,
+    cp_als_f64,
+    mttkrp_f64,
     cp_als_accelerated,
     cp_als_accelerated_dev,
     default_context,

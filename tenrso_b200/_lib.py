@@ -95,6 +95,9 @@ SIGNATURES = {
     "tsr_nmode_products_seq_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P, P]),
     "tsr_tucker_operator_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P, P]),
     "tsr_tucker_reconstruct_f32": (C.c_int, [P, P, C.c_int, P, C.c_int, P, P, P, P, P]),
+    "tsr_mttkrp_f64": (C.c_int, [P, P, C.c_int, P, P, C.c_int, P, P, C.c_int, P]),
+    "tsr_cp_als_f64": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_double, P, C.c_uint64,
+                                 C.c_double, P, C.POINTER(CpInfo)]),
     "tsr_cp_init_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_uint64, P]),
     "tsr_cp_init_dev_f32": (C.c_int, [P, P, C.c_int, P, I64, C.c_int, C.c_uint64, P]),
     "tsr_coo_sort_f32": (C.c_int, [P, P, P, I64, C.c_int, P]),

@@ -56,6 +56,7 @@ void init_adjoint_attributes();
 void init_batched_attributes();
 void init_accel_attributes();
 void init_init_attributes();
+void init_f64_attributes();
 
 // SplitMix64 U(0,1) stream identical to tenrso_b200.synth.uniform (the
 // library's InitStrategy::Random).

@@ -673,6 +673,7 @@ void init_kernel_attributes() {
   init_accel_attributes();
   init_hicoo_attributes();
   init_init_attributes();
+  init_f64_attributes();
   done_mask |= 1ull << dev;
 }
 

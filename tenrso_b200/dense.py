@@ -378,6 +378,55 @@ def cp_als_accelerated_dev(d_tensor: int, shape, rank: int, max_iters: int, tol:
     return float(info.fit), int(info.iters), _info_to(info, hist)
 
 
+def mttkrp_f64(tensor, factors: Sequence[np.ndarray], mode: int,
+               ctx: Optional[Context] = None) -> np.ndarray:
+    """mttkrp<f64> (mttkrp.rs:74-146): FP64 tensor, factors and result."""
+    t = np.ascontiguousarray(np.asarray(tensor, dtype=np.float64))
+    fs = [np.ascontiguousarray(np.asarray(f, dtype=np.float64)) for f in factors]
+    rows = _i64([f.shape[0] for f in fs] or [0])
+    cols = _i64([f.shape[1] if f.ndim == 2 else 0 for f in fs] or [0])
+    ptrs = (C.c_void_p * max(len(fs), 1))(*[f.ctypes.data for f in fs])
+    R = int(cols[0]) if len(fs) else 0
+    n_out = t.shape[mode] if 0 <= mode < t.ndim else 0
+    out = np.zeros((max(n_out, 1), max(R, 1)), np.float64)
+    check(_lib.load().tsr_mttkrp_f64(_ctx_handle(ctx), _ptr(t), t.ndim, _ptr(_i64(t.shape)), ptrs,
+                                     len(fs), _ptr(rows), _ptr(cols), mode, _ptr(out)))
+    return out[:n_out, :R]
+
+
+def cp_als_f64(tensor, rank: int, max_iters: int, tol: float, init="random",
+               time_limit: Optional[float] = None, seed: int = 0,
+               ctx: Optional[Context] = None) -> CpDecomp:
+    """cp_als<f64> (cp/core.rs:59-182): every value in FP64. init: "random"
+    (U(0,1) doubles from the seeded stream `seed`) or the initial factors."""
+    t = np.ascontiguousarray(np.asarray(tensor, dtype=np.float64))
+    total = int(sum(n * rank for n in t.shape))
+    out = np.zeros(max(total, 1), dtype=np.float64)
+    keep = None
+    if isinstance(init, str):
+        if init.lower() != "random":
+            keep = np.concatenate([np.asarray(f, np.float64).ravel() for f in
+                                   initialize_factors(t, rank, init, seed, ctx)])
+    else:
+        keep = np.concatenate([np.asarray(f, np.float64).ravel() for f in init])
+        if keep.size != total:
+            raise ValueError("initial factors do not match shape x rank")
+    hist = np.zeros(max(max_iters, 1), dtype=np.float64)
+    info = CpInfo()
+    info.fit_history = hist.ctypes.data_as(C.POINTER(C.c_double))
+    check(_lib.load().tsr_cp_als_f64(_ctx_handle(ctx), _ptr(t), t.ndim, _ptr(_i64(t.shape)), rank,
+                                     max_iters, float(tol),
+                                     _ptr(keep) if keep is not None else None, seed,
+                                     -1.0 if time_limit is None else float(time_limit),
+                                     _ptr(out), C.byref(info)))
+    factors, off = [], 0
+    for n in t.shape:
+        factors.append(out[off:off + n * rank].reshape(n, rank).copy())
+        off += n * rank
+    return CpDecomp(factors=factors, weights=None, fit=float(info.fit), iters=int(info.iters),
+                    convergence=_info_to(info, hist), ridge_used=bool(info.ridge_used))
+
+
 def profile_mttkrp_dev(d_tensor: int, shape, d_factors: Sequence[int], rank: int, mode: int,
                        precision="bf16x3", iters: int = 10, flush_l2: bool = True,
                        ctx: Optional[Context] = None):
