@@ -33,6 +33,9 @@ RANK = 64
 ITERS = 10
 SEED = 0xC2
 WORKLOAD = "dense CP-ALS 256x256x256 rank 64, 10 iterations, tol 0"
+# DRAM read + write bytes of one mode-0 launch of the single-layout BF16x3
+# MTTKRP at 256^3 rank 64 (ncu, dram__bytes_read.sum + dram__bytes_write.sum)
+MTTKRP3_TRAFFIC = 67_278_592 + 960_256
 
 
 def measured_peaks() -> dict:
@@ -288,22 +291,31 @@ CASES = {"mttkrp": case_mttkrp, "cp_als": case_cp_als, "csf_mttkrp": case_csf_mt
 
 
 # ---------------------------------------------------------------------------
+def cpu_cp_als_rate(X, init, iters: int = 1):
+    """Iterations/s of the oracle's restated cp_als<f32> (cp/core.rs:59-182) on
+    this box's host cores: the full loop (three mode updates with their
+    MTTKRPs, Gram Hadamards and solves, then the fit's extra MTTKRP), OpenMP
+    over all threads. Returns (iter/s, threads)."""
+    from oracle import oracle as orc
+    t0 = time.perf_counter()
+    orc.cp_als(X, RANK, iters, 0.0, init)
+    return iters / (time.perf_counter() - t0), orc.num_threads()
+
+
 def run_reference(args):
-    """The CPU restatement of tenrso's serial cp_als<f32> (oracle/, the
-    reference's own loop order: unfold copy, materialised Khatri-Rao, i/r/j
-    triple loop, per-row solve). One step = one of the four MTTKRP-based
-    updates of an iteration (mode 0 MTTKRP + Gram Hadamard + solve); an
-    iteration is four of them (three modes + the fit's extra MTTKRP)."""
+    """The CPU restatement of tenrso's cp_als<f32> (oracle/; the reference's
+    loop, solve and fit), on the host cores with every OpenMP thread. One step
+    = one full ALS iteration (modes 0..2 + fit) from the seeded init. Also
+    reported: the single-thread faithful restatement (unfold copy,
+    materialised Khatri-Rao, i/r/j loop) of one mode update, x4."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as orc
     X, init = make_inputs()
-    G = orc.gram(init[1]) * orc.gram(init[2])
 
     def step():
-        M = orc.mttkrp(X, init, 0, faithful=True)
-        orc.solve(M, G)
+        orc.cp_als(X, RANK, 1, 0.0, init)
 
     for _ in range(args.warmup):
         step()
@@ -311,16 +323,24 @@ def run_reference(args):
     for _ in range(args.steps):
         step()
     dt = (time.perf_counter() - t0) / args.steps
-    it_s = 1.0 / (4.0 * dt)
+    it_s = 1.0 / dt
+    G = orc.gram(init[1]) * orc.gram(init[2])
+    t1 = time.perf_counter()
+    orc.solve(orc.mttkrp(X, init, 0, faithful=True), G)
+    faithful = 1.0 / (4.0 * (time.perf_counter() - t1))
     line = {
         "impl": "reference", "metric": METRIC, "value": it_s, "unit": "iter/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
-        "config": {"workload": WORKLOAD, "sample": "one MTTKRP-based mode update per step"},
-        "cpu_baseline": {"value": it_s, "unit": "iter/s", "cores": 1, "kind": "port",
-                         "sample": "mode-0 MTTKRP + Gram-Hadamard + row solve of the faithful "
-                                   "f32 restatement, x4 per iteration"},
+        "config": {"workload": WORKLOAD, "sample": "one full ALS iteration per step"},
+        "cpu_baseline": {"value": it_s, "unit": "iter/s", "cores": orc.num_threads(),
+                         "kind": "port",
+                         "sample": "one full iteration of the restated cp_als<f32> "
+                                   "(OpenMP over all host threads) per step"},
+        "faithful_serial": {"value": faithful, "unit": "iter/s", "cores": 1,
+                            "sample": "one mode-0 update of the faithful single-thread "
+                                      "restatement, x4 per iteration"},
         "e2e": {"value": it_s, "unit": "iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -349,6 +369,13 @@ def run_sparse(tb, torch, ctx, stream, args, world, dist):
     t1 = time.perf_counter()
     n = tb.coo_deduplicate_dev(d_idx.data_ptr(), d_val.data_ptr(), n_raw, SP_SHAPE, ctx=ctx)
     t2 = time.perf_counter()
+    cpu_sample = None
+    if world == 1 and not args.no_cpu_baseline:
+        # the CPU baseline's sample: the merged entries of every 20th root
+        # (mode-0 index % 20 == 0; the Zipf head sits at permuted indices)
+        idx = d_idx[:3 * n].view(n, 3)
+        keep = idx[:, 0] % 20 == 0
+        cpu_sample = (idx[keep].cpu().numpy(), d_val[:n][keep].cpu().numpy())
     sp = tb.SparseTensor(ctx=ctx, d_indices=d_idx.data_ptr(), d_values=d_val.data_ptr(), nnz=n,
                          shape=SP_SHAPE)
     t3 = time.perf_counter()
@@ -383,13 +410,49 @@ def run_sparse(tb, torch, ctx, stream, args, world, dist):
                       "fibers": inf["fibers"], "bytes_min": b_min,
                       "achieved_gbs": b_min / (kms * 1e-3) / 1e9})
     sp.close()
+    cpu = None
+    if cpu_sample is not None:
+        cpu = csf_cpu_baseline(cpu_sample, n, modes[0]["kernel_ms"])
     return {"workload": f"CSF CP-ALS {SP_SHAPE[0]}x{SP_SHAPE[1]}x{SP_SHAPE[2]}, Zipf(1.2) indices "
                         f"over seeded permutations, rank {SP_RANK}, {SP_ITERS} iterations",
             "nnz": n, "raw_entries": n_raw, "duplicates_merged": n_raw - n,
             "iter_per_s": iters * world / (ms / 1e3), "ms_per_run": ms, "fit": fit,
             "iters": iters, "synth_s": t1 - t0, "dedup_s": t2 - t1, "csf_build_s": t3 - t2,
             "mttkrp": modes,
-            "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / hbm_peak_gbs()}
+            "mttkrp_hbm_frac_mean": float(np.mean([m["achieved_gbs"] for m in modes])) / hbm_peak_gbs(),
+            "cpu_baseline": cpu}
+
+
+def csf_cpu_baseline(sample, nnz_total: int, gpu_mode0_ms: float):
+    """The restated CSF MTTKRP (no tenrso implementation; oracle/) rooted at
+    mode 0 on the sampled entries, serial and OpenMP, as nnz/s, with the
+    mode-0 time at the full nnz it implies."""
+    from oracle import oracle as orc
+    idx, vals = sample
+    mo = [0, 2, 1]  # the root, then the other modes by ascending size
+    t0 = time.perf_counter()
+    fp, fi, v = orc.csf_from_coo(idx, vals, mo)
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(1)
+    fs = [rng.random((m, SP_RANK), dtype=np.float32) for m in SP_SHAPE]
+    out = {"kind": "port", "unit": "nnz/s", "sample_nnz": int(len(vals)),
+           "sample": "merged entries of every 20th mode-0 root; restated CSF MTTKRP rooted at "
+                     "mode 0 (mode order 0, 2, 1), fp32",
+           "csf_from_coo_s": build_s}
+    for label, threads in (("serial", 1), ("openmp", orc.num_threads())):
+        orc.csf_mttkrp(fp, fi, v, mo, SP_SHAPE, fs, threads)  # warm
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            orc.csf_mttkrp(fp, fi, v, mo, SP_SHAPE, fs, threads)
+        dt = (time.perf_counter() - t0) / reps
+        rate = len(vals) / dt
+        out[label] = {"value": rate, "cores": threads,
+                      "mode0_ms_at_full_nnz": nnz_total / rate * 1e3,
+                      "gpu_speedup_mode0": nnz_total / rate * 1e3 / gpu_mode0_ms}
+    out["value"] = out["openmp"]["value"]
+    out["cores"] = out["openmp"]["cores"]
+    return out
 
 
 AD_SHAPE = (128, 96, 64, 48)
@@ -620,14 +683,14 @@ def run_ours(args):
     peaks = measured_peaks()
     peak = hbm_peak_gbs()
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
-    # DRAM bytes (read + write) of one launch of this kernel, mode 0, from an
-    # ncu capture of `bench.py --case mttkrp --precision bf16x3 --mode 0` (the
-    # three modes move the same bytes at this shape)
-    traffic = 67_304_192 + 788_480
+    # DRAM bytes (read + write) of one launch of the kernel, mode 0, from an
+    # ncu capture of `bench.py --case mttkrp --precision bf16x3 --mode 0`
+    traffic = MTTKRP3_TRAFFIC
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes",
                 "algorithmic_bytes": alg_bytes,
-                "kernel": "mttkrp_bf16x3_runs_kernel", "kernel_ms": kernel_ms,
+                "kernel": "mttkrp3_kernel", "kernel_ms": kernel_ms,
+                "kernel_ms_per_mode": kms,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
     # e2e through the host API: pinned host tensor in, factors out
@@ -655,15 +718,10 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        from oracle import oracle as orc
-        G = orc.gram(init[1]) * orc.gram(init[2])
-        t0 = time.perf_counter()
-        M = orc.mttkrp(X, init, 0, faithful=True)
-        orc.solve(M, G)
-        dt = time.perf_counter() - t0
-        cpu = {"value": 1.0 / (4.0 * dt), "unit": "iter/s", "cores": 1, "kind": "port",
-               "sample": "one mode-0 MTTKRP + Gram-Hadamard + solve of the faithful serial "
-                         "f32 restatement of cp_als on the same tensor, x4 per iteration"}
+        rate, threads = cpu_cp_als_rate(X, init, 2)
+        cpu = {"value": rate, "unit": "iter/s", "cores": threads, "kind": "port",
+               "sample": "two full iterations of the restated cp_als<f32> (OpenMP over all "
+                         "host threads) on the same tensor and init"}
 
     if dist is not None:
         dist.barrier()

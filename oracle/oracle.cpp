@@ -596,6 +596,50 @@ double orc_cp_slice_sqerr_f64(const double* X, int ndim, const int64_t* shape,
   return acc;
 }
 
+// Restated CSF MTTKRP over the reference CSF layout (csf.rs:193-254: every
+// fptr level holds nnz offsets), 3-way, root = mode_order[0]; no tenrso
+// implementation exists (csf.rs:42). Per root: for each of its level-1 fibers
+// t = sum_k v_k U_leaf[leaf_k], then acc += U_fiber[fiber id] (*) t; the root's
+// row of out (zeroed here) receives acc. fp32 arithmetic, as the f32 path.
+// threads > 1 splits the roots over OpenMP threads (each output row has one
+// owner); threads == 1 runs the same loop serially.
+void orc_csf_mttkrp_f32(int64_t n_roots, const int64_t* root_ptr, const int64_t* root_ids,
+                        int64_t n_fibers, const int64_t* fib_ptr, const int64_t* fib_ids,
+                        const int64_t* leaf_ids, const float* vals, const float* U_fiber,
+                        const float* U_leaf, int64_t R, int64_t out_rows, float* out,
+                        int threads) {
+  std::fill(out, out + out_rows * R, 0.0f);
+  auto body = [&](int64_t s, std::vector<float>& acc, std::vector<float>& t) {
+    std::fill(acc.begin(), acc.end(), 0.0f);
+    const int64_t k0 = root_ptr[s], k1 = root_ptr[s + 1];
+    // first fiber of the root: fib_ptr[f] == k0
+    int64_t f = std::lower_bound(fib_ptr, fib_ptr + n_fibers, k0) - fib_ptr;
+    for (; f < n_fibers && fib_ptr[f] < k1; ++f) {
+      const int64_t e1 = f + 1 < n_fibers ? fib_ptr[f + 1] : k1;
+      std::fill(t.begin(), t.end(), 0.0f);
+      for (int64_t k = fib_ptr[f]; k < e1 && k < k1; ++k) {
+        const float* row = U_leaf + leaf_ids[k] * R;
+        for (int64_t r = 0; r < R; ++r) t[r] += vals[k] * row[r];
+      }
+      const float* urow = U_fiber + fib_ids[f] * R;
+      for (int64_t r = 0; r < R; ++r) acc[r] += urow[r] * t[r];
+    }
+    float* o = out + root_ids[s] * R;
+    for (int64_t r = 0; r < R; ++r) o[r] += acc[r];
+  };
+  if (threads <= 1) {
+    std::vector<float> acc(R), t(R);
+    for (int64_t s = 0; s < n_roots; ++s) body(s, acc, t);
+    return;
+  }
+#pragma omp parallel num_threads(threads)
+  {
+    std::vector<float> acc(R), t(R);
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t s = 0; s < n_roots; ++s) body(s, acc, t);
+  }
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

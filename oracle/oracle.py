@@ -55,6 +55,7 @@ def lib():
         L.orc_coo_dedup_f32.restype = I64
         L.orc_csf_from_coo_f32.argtypes = [P, P, I64, C.c_int, P, P, P, P, P]
         L.orc_coo_mttkrp_f64.argtypes = [P, P, I64, C.c_int, P, P, I64, C.c_int, P]
+        L.orc_csf_mttkrp_f32.argtypes = [I64, P, P, I64, P, P, P, P, P, P, I64, I64, P, C.c_int]
         L.orc_cp_reconstruct_f64.argtypes = [P, C.c_int, P, I64, P, P]
         L.orc_cp_slice_sqerr_f64.argtypes = [P, C.c_int, P, P, I64, C.c_int, I64]
         L.orc_cp_slice_sqerr_f64.restype = C.c_double
@@ -323,6 +324,23 @@ def hicoo_from_coo(idx, vals, block_shape):
     starts = np.flatnonzero(new)
     ptrs = np.append(starts, len(v)).astype(np.int64)
     return blk[starts], ptrs, loc, v
+
+
+def csf_mttkrp(fptr, fids, vals, mode_order, shape, factors, threads: int = 1):
+    """Restated 3-way CSF MTTKRP (fp32, rooted at mode_order[0]) over the
+    reference CSF arrays of csf_from_coo; threads > 1 runs the roots in
+    parallel (OpenMP), 1 serially. Returns the root mode's I x R result."""
+    fs = [np.ascontiguousarray(f, dtype=np.float32) for f in factors]
+    R = fs[0].shape[1]
+    mo = list(mode_order)
+    a = [np.ascontiguousarray(x, dtype=np.int64) for x in (fptr[0], fids[0], fptr[1], fids[1],
+                                                           fids[2])]
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    out = np.zeros((shape[mo[0]], R), np.float32)
+    lib().orc_csf_mttkrp_f32(len(a[1]), _ptr(a[0]), _ptr(a[1]), len(a[3]), _ptr(a[2]),
+                             _ptr(a[3]), _ptr(a[4]), _ptr(v), _ptr(fs[mo[1]]), _ptr(fs[mo[2]]), R,
+                             shape[mo[0]], _ptr(out), int(threads))
+    return out
 
 
 def coo_mttkrp(idx, vals, shape, factors, mode):

@@ -283,3 +283,20 @@ def test_oracle_reproduces_c2_accel_fixture(orc):
     init = [f.astype(np.float64) for f in synth.init_factors((256, 256, 256), 64, 0xC2)]
     _, info = orc.cp_als_accelerated(X.astype(np.float64), 64, 2, 1e-9, init)
     assert np.allclose(info["fit_history"], ref["fp64_fit_history"][:2], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+def test_csf_mttkrp_restatement_matches_coo_definition(orc, threads):
+    """The restated CSF MTTKRP (the C3 CPU baseline) against the FP64 COO
+    definition on a Zipf tensor, rooted at every mode."""
+    shape = (300, 200, 100)
+    idx, vals, _ = synth.zipf_coo(shape, 20000, 0xC3)
+    idx, vals = orc.coo_deduplicate(idx, vals)
+    rng = np.random.default_rng(2)
+    fs = [rng.random((n, 16), dtype=np.float32) for n in shape]
+    for root in range(3):
+        mo = [root] + sorted((m for m in range(3) if m != root), key=lambda m: shape[m])
+        fp, fi, v = orc.csf_from_coo(idx, vals, mo)
+        got = orc.csf_mttkrp(fp, fi, v, mo, shape, fs, threads)
+        ref = orc.coo_mttkrp(idx, vals, shape, fs, root)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-5
