@@ -426,7 +426,8 @@ int cp_als_accelerated_device(tsr_ctx* ctx, const float* dX, int ndim, const int
       TSR_TRY(prepare_mode(ctx, dX, ndim, shape, m, precision, m, &ops[m]));
       const bool tc = precision == TSR_PREC_BF16X3;
       const SplitPlan p = tc ? plan_tc(ctx, ops[m].u, R)
-                             : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
+                             : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R,
+                                         simt_run_len(ops[m]));
       pmax = std::max(pmax, partial_floats(p, ops[m].u.rows, R));
     }
     TSR_TRY(launch_norm_sq(ctx, ctx->stream, dX, n, (double*)xn_dev));

@@ -41,6 +41,8 @@ int prepare_mode_into(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* sh
 // Same, with buffers from the context's unfolding slots (slot_index 0..7).
 int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, int mode,
                  int precision, int slot_index, ModeOperand* op);
+// Run length of an FP32 operand for the run-scaled SIMT kernel (0: not usable).
+int64_t simt_run_len(const ModeOperand& op);
 // Split-K partial MTTKRP of one mode into the context's partial slot.
 int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& ft, int R,
                         int precision, float** partials, int* splits);

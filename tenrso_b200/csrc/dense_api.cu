@@ -175,6 +175,14 @@ int prepare_mode(tsr_ctx* ctx, const float* dX, int ndim, const int64_t* shape, 
 }
 
 // Split-K partial MTTKRP of one mode into `partials` (allocated here).
+// Run length of the FP32 operand for the run-scaled kernel (the fastest other
+// mode), or 0 when its rows are not 16-byte aligned.
+int64_t simt_run_len(const ModeOperand& op) {
+  if (!op.f32 || ((uintptr_t)op.f32 & 15) != 0 || (op.u.ld & 3) != 0 || op.u.n_other < 1)
+    return 0;
+  return op.u.other_size[op.u.n_other - 1];
+}
+
 int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& ft, int R,
                         int precision, float** partials, int* splits) {
   KRSpec kr = make_krspec(op.u, ft, R);
@@ -182,7 +190,8 @@ int run_mttkrp_partials(tsr_ctx* ctx, const ModeOperand& op, const FactorTable& 
   bool tc = precision == TSR_PREC_BF16X3;
   if (tc && !tc_supported(op.u, R))
     return fail(TSR_E_UNSUPPORTED, "BF16X3 path needs rank <= 256 (got %d)", R);
-  plan = tc ? plan_tc(ctx, op.u, R) : plan_simt(ctx, op.u.rows, op.u.cols, R);
+  plan = tc ? plan_tc(ctx, op.u, R)
+            : plan_simt(ctx, op.u.rows, op.u.cols, R, simt_run_len(op));
   void* p;
   TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * partial_floats(plan, op.u.rows, R), &p));
   if (tc)
@@ -516,7 +525,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
       }
       const bool tc = precision == TSR_PREC_BF16X3;
       SplitPlan p = tc ? plan_tc(ctx, ops[m].u, R)
-                       : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R);
+                       : plan_simt(ctx, ops[m].u.rows, ops[m].u.cols, R, simt_run_len(ops[m]));
       pmax = std::max(pmax, partial_floats(p, ops[m].u.rows, R));
       ops[m].resident = true;  // prepared here, before the sweep is enqueued
       a.op_ptrs[3 * m] = ops[m].f32;

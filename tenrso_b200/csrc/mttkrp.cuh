@@ -8,14 +8,18 @@ struct SplitPlan {
   int splits = 1;
   int64_t k_per_split = 0;
   int bn = 64;  // FP32 path: output columns per CTA tile (32 or 64)
-  int run_length = 0;  // BF16x3 path: > 0 selects the prefix-scaled kernel (runs of this length)
+  int run_length = 0;  // > 0 selects the run-scaled kernel (runs of this length), either path
 };
 
 void init_tc_attributes();
 void init_simt_attributes();
 
 // FP32 SIMT kernel (mttkrp_simt.cu).
-SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R);
+// L > 0: the unfolding's columns come in runs of L (the fastest other mode);
+// where the run-scaled kernel applies (L a multiple of 4, R <= 64, its
+// shared-memory tile fits) the plan selects it (run_length = L) and
+// k_per_split then counts 32-column steps over all runs.
+SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R, int64_t L = 0);
 int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
                        const SplitPlan& plan, float* partials);
 int launch_mttkrp_reduce(tsr_ctx* ctx, const float* partials, int splits, int64_t n, float* out);

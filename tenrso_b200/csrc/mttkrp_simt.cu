@@ -185,6 +185,146 @@ mttkrp_f32_splitk_kernel(const float* __restrict__ A, int64_t rows, int64_t K, i
   }
 }
 
+// Run-scaled FP32 form (the unfolding's columns come in runs of L, the size
+// of the fastest other mode): the Khatri-Rao rows of run P are U_last scaled
+// column-wise by w_P, the product of the slower modes' factor rows, so
+//   M = sum_P (X_P . U_last) diag(w_P)
+// with X_P the L columns of run P. U_last (L x BN) stays in shared memory for
+// the CTA's whole range of runs; no Khatri-Rao row is formed. The X tiles
+// (128 rows x 32 columns) stream in through cp.async, double-buffered. Each
+// thread owns rows ty + TY i and 4 columns; a run's products collect in
+// `acc`, which is scaled by w_P into `tot` where the run (or the CTA's range)
+// ends. The split-K ranges are counted in 32-column steps over all runs, so
+// the CTAs get equal work whether or not the runs divide evenly.
+constexpr int RUN_BM = 128, RUN_PITCH = 36;  // A tile rows, floats per staged row
+constexpr int kRunMaxSmem = 110 * 1024;      // two CTAs per SM
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;  // 0: zero-fill the 16 bytes
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(256, 2)
+mttkrp_f32_runs_kernel(const float* __restrict__ A, int64_t rows, int64_t ld, int L, int Lp,
+                       int64_t n_runs, int64_t steps_per_split, KRSpec kr,
+                       const float* __restrict__ UL, float* __restrict__ partials) {
+  constexpr int TX = BN / 4, TY = 256 / TX, RPT = RUN_BM / TY;
+  extern __shared__ __align__(16) float run_smem[];
+  float* Us = run_smem;                                   // Lp x BN
+  float (*As)[RUN_BM][RUN_PITCH] =
+      reinterpret_cast<float (*)[RUN_BM][RUN_PITCH]>(run_smem + (size_t)Lp * BN);
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int64_t m0 = (int64_t)blockIdx.y * RUN_BM;
+  const int n0 = blockIdx.z * BN;
+  const int R = kr.R;
+  const int steps_per_run = Lp / 32;
+  const int64_t g_begin = (int64_t)blockIdx.x * steps_per_split;
+  const int64_t g_end = min(n_runs * steps_per_run, g_begin + steps_per_split);
+  // U_last's columns n0..n0+BN-1, zero past L and past R
+  for (int e = tid; e < Lp * BN; e += 256) {
+    const int k = e / BN, c = e % BN;
+    Us[e] = (k < L && n0 + c < R) ? __ldg(UL + (int64_t)k * R + n0 + c) : 0.f;
+  }
+  // global step g's tile: 128 rows x 32 columns of run g / steps_per_run
+  auto issue = [&](int64_t g, int buf) {
+    const int64_t P = g / steps_per_run;
+    const int k0 = (int)(g % steps_per_run) * 32;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int idx = it * 256 + tid, r = idx / 8, kq = idx % 8;
+      const int64_t gm = m0 + r;
+      const int k = k0 + kq * 4;
+      const bool ok = gm < rows && k < L;
+      cp_async16(&As[buf][r][kq * 4], ok ? A + gm * ld + P * L + k : A, ok);
+    }
+    cp_async_commit();
+  };
+  float tot[RPT][4], acc[RPT][4];
+#pragma unroll
+  for (int i = 0; i < RPT; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tot[i][j] = acc[i][j] = 0.f;
+  float w[4] = {0.f, 0.f, 0.f, 0.f};
+  if (g_begin < g_end) issue(g_begin, 0);
+  for (int64_t g = g_begin; g < g_end; ++g) {
+    const int buf = (int)((g - g_begin) & 1);
+    const int kstep = (int)(g % steps_per_run);
+    if (kstep == 0 || g == g_begin) {
+      // this run's weights: the slower modes' factor rows
+      const int64_t P = g / steps_per_run;
+      uint32_t off[kMaxModes];
+      kr_row_offsets(kr, (uint32_t)(P * L), off);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = n0 + tx * 4 + j;
+        float v = c < R ? 1.f : 0.f;
+#pragma unroll
+        for (int q = 0; q < kMaxModes - 1; ++q)
+          if (q < kr.n_other - 1 && c < R) v *= __ldg(kr.f[q] + off[q] + c);
+        w[j] = v;
+      }
+    }
+    if (g + 1 < g_end) {
+      issue(g + 1, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const float* ub = Us + (size_t)kstep * 32 * BN + tx * 4;
+#pragma unroll 2
+    for (int kq = 0; kq < 8; ++kq) {
+      float4 a[RPT];
+#pragma unroll
+      for (int i = 0; i < RPT; ++i)
+        a[i] = *reinterpret_cast<const float4*>(&As[buf][ty + TY * i][kq * 4]);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const float4 b = *reinterpret_cast<const float4*>(ub + (kq * 4 + t) * BN);
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+          const float av = t == 0 ? a[i].x : (t == 1 ? a[i].y : (t == 2 ? a[i].z : a[i].w));
+          acc[i][0] = fmaf(av, b.x, acc[i][0]);
+          acc[i][1] = fmaf(av, b.y, acc[i][1]);
+          acc[i][2] = fmaf(av, b.z, acc[i][2]);
+          acc[i][3] = fmaf(av, b.w, acc[i][3]);
+        }
+      }
+    }
+    __syncthreads();  // the buffer is refilled two steps on
+    if (kstep == steps_per_run - 1 || g + 1 == g_end) {
+#pragma unroll
+      for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          tot[i][j] = fmaf(acc[i][j], w[j], tot[i][j]);
+          acc[i][j] = 0.f;
+        }
+    }
+  }
+  float* P = partials + (int64_t)blockIdx.x * rows * R;
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int64_t gm = m0 + ty + TY * i;
+    if (gm >= rows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = n0 + tx * 4 + j;
+      if (c < R) P[gm * R + c] = tot[i][j];
+    }
+  }
+}
+
 // out[e] = sum over splits of partials[s][e] (FP64), optionally times w[e % R].
 // `groups` threads share an element, each summing every groups-th split with
 // four loads in flight; the groups combine through shared memory.
@@ -246,6 +386,10 @@ constexpr size_t simt_smem_bytes() {
 }
 
 void init_simt_attributes() {
+  cudaFuncSetAttribute(mttkrp_f32_runs_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kRunMaxSmem);
+  cudaFuncSetAttribute(mttkrp_f32_runs_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kRunMaxSmem);
   cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 64, 2>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 64>());
   cudaFuncSetAttribute(mttkrp_f32_splitk_kernel<128, 64, 4>,
@@ -256,9 +400,35 @@ void init_simt_attributes() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<128, 32>());
 }
 
-SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R) {
+// Shared memory of the run-scaled kernel: U_last (Lp x BN) and two A tiles.
+template <int BN>
+constexpr size_t runs_smem_bytes(int Lp) {
+  return sizeof(float) * ((size_t)Lp * BN + 2 * RUN_BM * RUN_PITCH);
+}
+
+bool simt_runs_ok(int64_t L, int64_t K, int R) {
+  if (L < 16 || L % 4 != 0 || K % L != 0 || R < 1 || R > 64) return false;
+  const int64_t Lp = round_up(L, 32);
+  const size_t smem = R <= 32 ? runs_smem_bytes<32>((int)Lp) : runs_smem_bytes<64>((int)Lp);
+  return smem <= (size_t)kRunMaxSmem;
+}
+
+SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R, int64_t L) {
   SplitPlan p;
   p.bn = R <= 32 ? 32 : 64;
+  if (L > 0 && simt_runs_ok(L, K, R)) {
+    // equal ranges of 32-column steps (k_per_split counts steps here), one
+    // full wave at two CTAs per SM
+    const int64_t mt = ceil_div(rows, RUN_BM), nt = ceil_div(R, p.bn);
+    const int64_t steps = (K / L) * (round_up(L, 32) / 32);
+    const int64_t want = std::max<int64_t>(
+        1, std::min<int64_t>(steps, (int64_t)(ctx->sm_count - ctx->reserve_sms) * 2 / (mt * nt)));
+    const int64_t per = ceil_div(steps, want);
+    p.run_length = (int)L;
+    p.k_per_split = per;
+    p.splits = (int)ceil_div(steps, per);
+    return p;
+  }
   const int64_t mt = ceil_div(rows, 128), nt = ceil_div(R, p.bn);
   // one full wave at the resident CTAs per SM (2 of 256 threads, 4 of 128)
   const int per_sm = p.bn == 32 ? 4 : 2;
@@ -282,6 +452,27 @@ void launch_simt_tile(tsr_ctx* ctx, const float* A, const Unfolding& u, const KR
 int launch_mttkrp_simt(tsr_ctx* ctx, const float* A, const Unfolding& u, const KRSpec& kr,
                        const SplitPlan& plan, float* partials) {
   if (u.cols >= (int64_t)UINT32_MAX) return fail(TSR_E_UNSUPPORTED, "unfolding too wide");
+  if (plan.run_length > 0) {
+    // 16-byte cp.async sources need an aligned base and row stride (the plan
+    // only selects this kernel for such operands)
+    if (((uintptr_t)A & 15) != 0 || (u.ld & 3) != 0)
+      return fail(TSR_E_INVALID_ARG, "run-scaled FP32 MTTKRP needs 16-byte aligned rows");
+    const int L = plan.run_length, Lp = (int)round_up(L, 32);
+    const int64_t runs = u.cols / L;
+    const int64_t per = plan.k_per_split;  // 32-column steps per split
+    const int bn = plan.bn == 32 ? 32 : 64;
+    dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, RUN_BM), (unsigned)ceil_div(kr.R, bn));
+    if (grid.y > 65535 || grid.z > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
+    if (bn == 32)
+      mttkrp_f32_runs_kernel<32><<<grid, 256, runs_smem_bytes<32>(Lp), ctx->stream>>>(
+          A, u.rows, u.ld, L, Lp, runs, per, kr, kr.f[kr.n_other - 1], partials);
+    else
+      mttkrp_f32_runs_kernel<64><<<grid, 256, runs_smem_bytes<64>(Lp), ctx->stream>>>(
+          A, u.rows, u.ld, L, Lp, runs, per, kr, kr.f[kr.n_other - 1], partials);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    return TSR_OK;
+  }
   const int bn = plan.bn == 32 ? 32 : 64;
   dim3 grid(plan.splits, (unsigned)ceil_div(u.rows, 128), (unsigned)ceil_div(kr.R, bn));
   if (grid.y > 65535 || grid.z > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
