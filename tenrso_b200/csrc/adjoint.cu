@@ -27,9 +27,17 @@ struct tsr_dense {
   int precision = 0;
   int device = 0;
   const float* dX = nullptr;
-  void* owned[2 * tsr::kMaxModes] = {};
+  void* owned[2 * tsr::kMaxModes + 2] = {};
   tsr::ModeOperand ops[tsr::kMaxModes];
-  double* d_scalars = nullptr;  // [0] ||X||^2, [1] <X, Xhat>, [2] loss
+  double* d_scalars = nullptr;  // [0] ||X||^2, [1] <X, Xhat>, [2] loss, [3] scratch
+  // BF16x3 tensors of 4 or more modes whose trailing-two-modes view
+  // (prod of the leading modes, I_{N-2}, I_{N-1}) suits the two-sided
+  // contraction or the single-layout 3-way MTTKRP: X's bf16 halves in its own
+  // layout (owned[2N], owned[2N+1])
+  bool d3_on = false;
+  bool d3_three = false;  // the view suits the single-layout 3-way MTTKRP
+  bool d3_two = false;    // the view suits the two-sided contraction
+  tsr::Dense3 d3{};
 };
 
 namespace tsr {
@@ -259,6 +267,87 @@ __global__ void gram_loss_kernel(const double* __restrict__ grams, int ndim, int
   double t = 0.0;
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
   scal[2] = scal[0] - 2.0 * scal[1] + t;
+}
+
+// MTTKRPs from a partial contraction. A side holds S (rows a over nlead
+// modes, row-major, fewer than 2^31 rows) with
+//   S[a, r] = sum over the other modes of X[a, ...] prod_{other p} U_p[., r],
+// and the mode-m MTTKRP of one of its modes is
+//   M_m[i, r] = sum_{a : a_m = i} S[a, r] prod_{p in side, p != m} U_p[a_p, r].
+// The leading modes 0..N-3 come from T (S over the leading modes, the
+// trailing two contracted), the trailing two from P (S over (I_{N-2},
+// I_{N-1}), the leading modes contracted). One launch for every requested
+// mode: block b is row i of mode n (the modes' rows stacked in `out`), lane r
+// of a group of R threads, the groups split the side's other indices; FP64
+// sums, fp32 output.
+struct TSideC {
+  const float* S;
+  int nlead;
+  int arows;
+  int size[kMaxModes];
+  int stride[kMaxModes];
+  const float* U[kMaxModes];
+};
+
+struct TContract {
+  TSideC side[2];
+  int R, nmodes;
+  int side_of[kMaxModes];  // output mode -> side
+  int pos[kMaxModes];      // output mode -> its index within the side
+  int row0[kMaxModes + 1];
+  float* out;
+};
+
+__global__ void __launch_bounds__(256) t_contract_kernel(const __grid_constant__ TContract c) {
+  __shared__ double part[256];
+  const int b = blockIdx.x;
+  int n = 0;
+  while (n + 1 < c.nmodes && b >= c.row0[n + 1]) ++n;
+  const TSideC& sd = c.side[c.side_of[n]];
+  const int m = c.pos[n];
+  const int i = b - c.row0[n];
+  const int R = c.R;
+  const int groups = blockDim.x / R;
+  const int g = threadIdx.x / R, r = threadIdx.x % R;
+  double s = 0.0;
+  if (g < groups) {
+    const int count = sd.arows / sd.size[m];
+    for (int q = g; q < count; q += groups) {
+      int rem = q, a = i * sd.stride[m];
+      double w = 1.0;
+      for (int p = sd.nlead - 1; p >= 0; --p) {
+        if (p == m) continue;
+        const int ip = rem % sd.size[p];
+        rem /= sd.size[p];
+        a += ip * sd.stride[p];
+        w *= (double)__ldg(sd.U[p] + (int64_t)ip * R + r);
+      }
+      s += (double)__ldg(sd.S + (int64_t)a * R + r) * w;
+    }
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < R) {
+    double t = 0.0;
+    for (int q = 0; q < groups; ++q) t += part[q * R + threadIdx.x];
+    c.out[(int64_t)b * R + threadIdx.x] = (float)t;
+  }
+}
+
+// side k of c over modes m0 .. m1-1 of the tensor, the partial contraction S
+void set_side(TContract& c, int k, const float* S, const int64_t* shape, int m0, int m1,
+              const float* const* U) {
+  TSideC& sd = c.side[k];
+  sd.S = S;
+  sd.nlead = m1 - m0;
+  int st = 1;
+  for (int p = m1 - 1; p >= m0; --p) {
+    sd.size[p - m0] = (int)shape[p];
+    sd.stride[p - m0] = st;
+    sd.U[p - m0] = U[p];
+    st *= (int)shape[p];
+  }
+  sd.arows = st;
 }
 
 int64_t prod_range(const int64_t* shape, int m0, int m1) {
@@ -560,6 +649,31 @@ int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, cons
   }
   if (cudaMalloc(&d->d_scalars, 4 * sizeof(double)) != cudaSuccess)
     return cleanup(fail(TSR_E_CUDA, "cudaMalloc of the loss scalars failed"));
+  // BF16x3, 4+ modes: the trailing-two-modes view for the single-layout kernel
+  const int64_t vshape[3] = {prod_range(shape, 0, ndim - 2), shape[ndim - 2], shape[ndim - 1]};
+  d->d3_three = dense3_supported(3, vshape, 1);
+  d->d3_two = twosided_supported(vshape[0], vshape[1] * vshape[2], 1);
+  if (precision == TSR_PREC_BF16X3 && ndim >= 4 && (d->d3_three || d->d3_two) &&
+      vshape[0] <= ((int64_t)1 << 30) &&
+      ((uintptr_t)d_tensor & 15) == 0) {
+    const int64_t n = numel(ndim, shape);
+    void *hp, *lp;
+    if (cudaMalloc(&hp, sizeof(__nv_bfloat16) * n) != cudaSuccess)
+      return cleanup(fail(TSR_E_CUDA, "cudaMalloc of the bf16 halves failed"));
+    d->owned[2 * kMaxModes] = hp;
+    if (cudaMalloc(&lp, sizeof(__nv_bfloat16) * n) != cudaSuccess)
+      return cleanup(fail(TSR_E_CUDA, "cudaMalloc of the bf16 halves failed"));
+    d->owned[2 * kMaxModes + 1] = lp;
+    int rc = launch_split_bf16(ctx, ctx->stream, d_tensor, n, (__nv_bfloat16*)hp,
+                               (__nv_bfloat16*)lp, d->d_scalars + 3);
+    if (rc != TSR_OK) return cleanup(rc);
+    d->d3_on = true;
+    d->d3.I = vshape[0];
+    d->d3.J = vshape[1];
+    d->d3.K = vshape[2];
+    d->d3.hi = (const __nv_bfloat16*)hp;
+    d->d3.lo = (const __nv_bfloat16*)lp;
+  }
   cudaError_t e = cudaMemsetAsync(d->d_scalars, 0, 4 * sizeof(double), ctx->stream);
   if (e != cudaSuccess) return cleanup(fail(TSR_E_CUDA, "%s", cudaGetErrorString(e)));
   int rc = launch_norm_sq(ctx, ctx->stream, d_tensor, numel(ndim, shape), d->d_scalars);
@@ -607,6 +721,170 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     TSR_TRY(launch_gram(ctx, ctx->stream, d_factors[m], X->shape[m], R, grams + (size_t)m * RR,
                         true));
   TSR_CUDA(cudaMemsetAsync(X->d_scalars + 1, 0, 2 * sizeof(double), ctx->stream));
+  auto grad_of = [&](int n, const float* partials, int splits) -> int {
+    const int64_t rows = X->shape[n];
+    const int rpc =
+        (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 2 * ctx->sm_count)));
+    const int full = rpc * R;
+    const int groups = full >= 256 ? 1 : 256 / full;
+    const size_t smem = sizeof(double) * ((size_t)RR + full + (size_t)groups * full);
+    if (smem > 200 * 1024)
+      return fail(TSR_E_UNSUPPORTED, "rank %d too large for the gradient kernel", R);
+    gram_grad_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, ctx->stream>>>(
+        grams, N, n, partials, splits, rows, R, rpc, d_factors[n], reg, d_grads[n],
+        X->d_scalars);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    return TSR_OK;
+  };
+  auto finish = [&]() -> int {
+    gram_loss_kernel<<<1, 256, 0, ctx->stream>>>(grams, N, R, reg, X->d_scalars);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    TSR_TRY(check_device_status(ctx));
+    if (loss) {
+      TSR_CUDA(cudaMemcpyAsync(loss, X->d_scalars + 2, sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return TSR_OK;
+  };
+  if (X->d3_on && X->d3_two && twosided_supported(X->d3.I, X->d3.J * X->d3.K, R)) {
+    // one read of X's bf16 halves: T = X_(lead) KR(trailing two) and
+    // P = X_(lead)^T KR(leading) from the two-sided contraction, then every
+    // mode's MTTKRP from T (modes 0..N-3) or P (modes N-2, N-1)
+    const int64_t A = X->d3.I, C = X->d3.J * X->d3.K;
+    const int64_t Ap = twosided_pad(A), Cp = twosided_pad(C);
+    void *kp, *kq, *wp, *tp, *mp, *ip;
+    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * A * R, &kp));
+    TSR_TRY(slot_get(ctx, SLOT_MISC3, sizeof(float) * A * R, &kq));
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * C * R, &wp));
+    const float* kr = d_factors[0];
+    int64_t krows = X->shape[0];
+    float* bufs[2] = {(float*)kp, (float*)kq};
+    for (int p = 1; p < N - 2; ++p) {
+      float* dst = bufs[p & 1];
+      TSR_TRY(launch_khatri_rao(ctx, kr, krows, d_factors[p], X->shape[p], R, dst));
+      kr = dst;
+      krows *= X->shape[p];
+    }
+    TSR_TRY(launch_khatri_rao(ctx, d_factors[N - 2], X->d3.J, d_factors[N - 1], X->d3.K, R,
+                              (float*)wp));
+    const size_t vb = bimage_bytes(Ap, 32), wb = bimage_bytes(Cp, 32);
+    TSR_TRY(slot_get(ctx, SLOT_D3_IMG, vb + wb, &ip));
+    TSR_TRY(launch_bimage(ctx, ctx->stream, kr, A, R, 32, (uint8_t*)ip, Ap));
+    TSR_TRY(launch_bimage(ctx, ctx->stream, (const float*)wp, C, R, 32, (uint8_t*)ip + vb, Cp));
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * (A + C) * R, &tp));
+    TSR_CUDA(cudaMemsetAsync(tp, 0, sizeof(float) * (A + C) * R, ctx->stream));
+    TwoSided ts;
+    ts.hi = X->d3.hi;
+    ts.lo = X->d3.lo;
+    ts.A = A;
+    ts.C = C;
+    ts.R = R;
+    ts.vimg = (const uint8_t*)ip;
+    ts.wimg = (const uint8_t*)ip + vb;
+    ts.T = (float*)tp;
+    ts.P = (float*)tp + A * R;
+    TSR_TRY(launch_twosided(ctx, ctx->stream, ts));
+    int total_rows = 0;
+    for (int p = 0; p < N; ++p) total_rows += (int)X->shape[p];
+    TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(float) * total_rows * R, &mp));
+    TContract c{};
+    set_side(c, 0, ts.T, X->shape, 0, N - 2, d_factors);
+    set_side(c, 1, ts.P, X->shape, N - 2, N, d_factors);
+    c.R = R;
+    c.nmodes = N;
+    c.row0[0] = 0;
+    for (int p = 0; p < N; ++p) {
+      c.side_of[p] = p < N - 2 ? 0 : 1;
+      c.pos[p] = p < N - 2 ? p : p - (N - 2);
+      c.row0[p + 1] = c.row0[p] + (int)X->shape[p];
+    }
+    c.out = (float*)mp;
+    t_contract_kernel<<<(unsigned)total_rows, 256, 0, ctx->stream>>>(c);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    for (int m = 0; m < N; ++m)
+      TSR_TRY(grad_of(m, (const float*)mp + (int64_t)c.row0[m] * R, 1));
+    return finish();
+  }
+  if (X->d3_on && X->d3_three && R <= 64) {
+    // three single-layout passes over X's bf16 halves instead of one MTTKRP
+    // per mode: the view (A = prod of the leading modes, I_{N-2}, I_{N-1})
+    Dense3 d = X->d3;
+    d.R = R;
+    d.n_pad = dense3_n_pad(R);
+    const int64_t A = d.I;
+    // Khatri-Rao of the leading factors (forward order): the view's U0
+    void *kp, *kq, *tp, *mp, *ip;
+    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * A * R, &kp));
+    TSR_TRY(slot_get(ctx, SLOT_MISC3, sizeof(float) * A * R, &kq));
+    const float* kr = d_factors[0];
+    int64_t krows = X->shape[0];
+    float* bufs[2] = {(float*)kp, (float*)kq};
+    for (int p = 1; p < N - 2; ++p) {
+      float* dst = bufs[p & 1];
+      TSR_TRY(launch_khatri_rao(ctx, kr, krows, d_factors[p], X->shape[p], R, dst));
+      kr = dst;
+      krows *= X->shape[p];
+    }
+    const size_t img1 = bimage_bytes(d.J, d.n_pad), img2 = bimage_bytes(d.K, d.n_pad);
+    TSR_TRY(slot_get(ctx, SLOT_D3_IMG, img1 + img2, &ip));
+    d.bimg[0] = nullptr;
+    d.bimg[1] = (uint8_t*)ip;
+    d.bimg[2] = (uint8_t*)ip + img1;
+    TSR_TRY(launch_bimage(ctx, ctx->stream, d_factors[N - 2], d.J, R, d.n_pad, d.bimg[1]));
+    TSR_TRY(launch_bimage(ctx, ctx->stream, d_factors[N - 1], d.K, R, d.n_pad, d.bimg[2]));
+    FactorTable vt{};
+    vt.ptr[0] = kr;
+    vt.rows[0] = A;
+    vt.ptr[1] = d_factors[N - 2];
+    vt.rows[1] = d.J;
+    vt.ptr[2] = d_factors[N - 1];
+    vt.rows[2] = d.K;
+    size_t pmax = 0;
+    for (int v = 0; v < 3; ++v) {
+      const SplitPlan pl = plan_mttkrp3(ctx, d, v);
+      pmax = std::max(pmax, (size_t)pl.splits * dense3_rows(d, v) * R);
+    }
+    void* pp;
+    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * pmax, &pp));
+    float* partials = (float*)pp;
+    // T = the view's mode-0 MTTKRP (A x R), then the leading modes from it
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * A * R, &tp));
+    {
+      const SplitPlan pl = plan_mttkrp3(ctx, d, 0);
+      TSR_TRY(launch_mttkrp3(ctx, ctx->stream, d, 0, vt, pl, partials, true));
+      TSR_TRY(launch_mttkrp_reduce(ctx, partials, pl.splits, A * R, (float*)tp));
+    }
+    int lead_rows = 0;
+    for (int p = 0; p < N - 2; ++p) lead_rows += (int)X->shape[p];
+    TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(float) * lead_rows * R, &mp));
+    TContract c{};
+    set_side(c, 0, (const float*)tp, X->shape, 0, N - 2, d_factors);
+    c.R = R;
+    c.nmodes = N - 2;
+    c.row0[0] = 0;
+    for (int p = 0; p < N - 2; ++p) {
+      c.side_of[p] = 0;
+      c.pos[p] = p;
+      c.row0[p + 1] = c.row0[p] + (int)X->shape[p];
+    }
+    c.out = (float*)mp;
+    t_contract_kernel<<<(unsigned)lead_rows, 256, 0, ctx->stream>>>(c);
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    for (int m = 0; m < N - 2; ++m)
+      TSR_TRY(grad_of(m, (const float*)mp + (int64_t)c.row0[m] * R, 1));
+    // the trailing two modes straight from the view's modes 1 and 2
+    for (int v = 1; v <= 2; ++v) {
+      const SplitPlan pl = plan_mttkrp3(ctx, d, v);
+      TSR_TRY(launch_mttkrp3(ctx, ctx->stream, d, v, vt, pl, partials, true));
+      TSR_TRY(grad_of(N - 3 + v, partials, pl.splits));
+    }
+    return finish();
+  }
   for (int n = 0; n < N; ++n) {
     float* partials;
     int splits;

@@ -56,13 +56,33 @@ int64_t dense3_rows(const Dense3& d, int mode);
 int launch_split_bf16(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, __nv_bfloat16* hi,
                       __nv_bfloat16* lo, double* norm_sq);
 // The whole B image of U (L x R), zero padding included.
+// L_img > L: the image covers L_img rows, those from L on zero.
 int launch_bimage(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t L, int R, int n_pad,
-                  uint8_t* img);
+                  uint8_t* img, int64_t L_img = 0);
 // SplitPlan: splits, k_per_split = runs per split, run_length = contracted length.
 SplitPlan plan_mttkrp3(const tsr_ctx* ctx, const Dense3& d, int mode);
 // Partials [splits][rows][R] of mode `mode`; the weights come from ft.
 int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, const FactorTable& ft,
                    const SplitPlan& plan, float* partials, bool a_resident);
+
+// Two-sided contraction of X seen as an A x C matrix (its bf16 halves,
+// row-major): T += X W (A x R) and P += X^T V (C x R) in one read of X, for
+// R <= 32. W (C x R) and V (A x R) come as B images with n_pad 32 covering
+// twosided_pad(C) and twosided_pad(A) rows. T and P are added into (fp32
+// atomics): zero them first.
+struct TwoSided {
+  const __nv_bfloat16* hi;
+  const __nv_bfloat16* lo;
+  int64_t A, C;
+  int R;
+  const uint8_t* wimg;
+  const uint8_t* vimg;
+  float* T;
+  float* P;
+};
+bool twosided_supported(int64_t A, int64_t C, int R);
+int64_t twosided_pad(int64_t L);
+int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a);
 
 // Materialised two-factor Khatri-Rao product (the public khatri_rao API).
 int launch_khatri_rao(tsr_ctx* ctx, const float* A, int64_t I, const float* B, int64_t J,

@@ -541,6 +541,307 @@ int encode_map3(CUtensorMap* map, const __nv_bfloat16* base, const Dense3& d, in
   return TSR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Two-sided contraction of X seen as an A x C matrix (row-major bf16 halves,
+// C = the trailing modes' product): in one read of X,
+//   T = X W    (A x R; W is C x R)      the MTTKRP side of the leading modes
+//   P = X^T V  (C x R; V is A x R)      the MTTKRP side of the trailing modes
+// W and V enter as B images (hi | lo rows, n_pad = 32). A CTA owns TS_TA
+// consecutive 128-row blocks of A and a range of 128-column blocks of C; a
+// tile (128 a x 128 c) arrives as four TMA boxes (hi and lo, two 64-column
+// boxes each, 128-byte swizzle) plus the W image of its column block and the
+// V image of its row block. The same shared-memory tile is
+//   the K-major A operand of T's MMA (rows a, K = c), accumulated in TMEM
+//     over every column block of the CTA (one accumulator per row block);
+//   the MN-major A operand of P's MMA (rows c, K = a), accumulated over the
+//     CTA's row blocks, then added into P (fp32 vector atomics) per column
+//     block from a double-buffered accumulator.
+// BF16x3 as in the MTTKRP above: D += Xhi [Bhi | Blo], D += Xlo [Bhi | Blo],
+// the result column n is D[:, n] + D[:, 32 + n].
+// Warp 0 TMA producer, warp 1 TMEM and the MMA-issuing thread, warps 2..5
+// the epilogue. Every wait is bounded (DS_TIMEOUT, then a drain).
+constexpr int TS_BM = 128;
+constexpr int TS_BOX = 128 * 64 * 2;                 // one 64-column box, 16 KB
+constexpr int TS_NPAD = 32;
+constexpr int TS_BTILE = 2 * TS_NPAD * 128;          // one 64-k block of an image, 8 KB
+constexpr int TS_STAGE = 4 * TS_BOX + 4 * TS_BTILE;  // X hi, X lo, W and V images
+constexpr int TS_STAGES = 2;
+constexpr int TS_TA = 4;
+constexpr int TS_THREADS = 192;
+constexpr uint32_t TS_TMEM_COLS = 512;  // TS_TA T accumulators + 2 P buffers of 64
+constexpr size_t TS_SMEM = 1024 + (size_t)TS_STAGES * TS_STAGE + 8 * (2 * TS_STAGES + 6) + 16;
+
+struct TSParams {
+  int64_t A, C;
+  int R;
+  int nab, ncb;        // 128-row blocks of A, 128-column blocks of C
+  int cb_per_split;
+  const uint8_t* wimg;  // ncb * 2 image blocks
+  const uint8_t* vimg;  // nab * 2 image blocks
+  float* T;
+  float* P;
+  unsigned* status;
+  long long wait_budget;
+};
+
+__device__ __forceinline__ uint64_t evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* map, int32_t x,
+                                                 int32_t y, uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(sm100::smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(sm100::smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          sm100::smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(sm100::smem_u32(bar))
+      : "memory");
+}
+
+// rows row0 .. row0 + 31 (one per lane) of a 64-column accumulator, hh | cr
+// halves summed, added into out[row, 0 .. R-1] for row < rows
+__device__ __forceinline__ void ts_flush(uint32_t taddr, int64_t row, int64_t rows, int R,
+                                         float* out) {
+  using namespace sm100;
+  uint32_t rh[2][16], rc[2][16];
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    tmem_ld16_nowait(taddr + (uint32_t)(16 * g), rh[g]);
+    tmem_ld16_nowait(taddr + (uint32_t)(TS_NPAD + 16 * g), rc[g]);
+  }
+  tmem_wait_ld();
+  if (row >= rows) return;
+  float v[32];
+#pragma unroll
+  for (int g = 0; g < 2; ++g)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[16 * g + i] = __uint_as_float(rh[g][i]) + __uint_as_float(rc[g][i]);
+  float* o = out + row * R;
+  if ((R & 3) == 0) {
+#pragma unroll
+    for (int n = 0; n < 32; n += 4)
+      if (n < R) atomicAdd(reinterpret_cast<float4*>(o + n), make_float4(v[n], v[n + 1], v[n + 2], v[n + 3]));
+  } else {
+#pragma unroll
+    for (int n = 0; n < 32; ++n)
+      if (n < R) atomicAdd(o + n, v[n]);
+  }
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+twosided_kernel(const __grid_constant__ CUtensorMap map_hi,
+                const __grid_constant__ CUtensorMap map_lo, TSParams p) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+  constexpr int S = TS_STAGES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * TS_STAGE);
+  uint64_t* tma_full = bars;
+  uint64_t* empty = bars + S;
+  uint64_t* p_full = bars + 2 * S;       // [2]
+  uint64_t* p_empty = bars + 2 * S + 2;  // [2]
+  uint64_t* t_full = bars + 2 * S + 4;
+  uint64_t* mma_done = bars + 2 * S + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 6);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ab0 = (int)blockIdx.y * TS_TA;
+  const int nta = p.nab - ab0 < TS_TA ? p.nab - ab0 : TS_TA;
+  const int cb0 = (int)blockIdx.x * p.cb_per_split;
+  const int cleft = p.ncb - cb0;
+  const int nc = cleft <= 0 ? 0 : (cleft < p.cb_per_split ? cleft : p.cb_per_split);
+  const int nsteps = nta > 0 ? nc * nta : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&tma_full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&p_full[b], 1);
+      mbar_init(&p_empty[b], 4);
+    }
+    mbar_init(t_full, 1);
+    mbar_init(mma_done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    prefetch_tmap(&map_hi);
+    prefetch_tmap(&map_lo);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, TS_TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint64_t pol = evict_first_policy();  // every tile is read once
+      int issued_upto = 0;
+      for (int it = 0; it < nsteps; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!m3_wait(&empty[s], ph ^ 1u, abort_flag, p.wait_budget)) {
+          *abort_flag = 1;
+          atomicOr(p.status, DS_TIMEOUT);
+          break;
+        }
+        uint8_t* st = smem + (size_t)s * TS_STAGE;
+        const int cb = cb0 + it / nta, ab = ab0 + it % nta;
+        const int32_t x = cb * 128, y = ab * TS_BM;
+        mbar_arrive_expect_tx(&tma_full[s], (uint32_t)TS_STAGE);
+        tma_load_2d_hint(st, &map_hi, x, y, &tma_full[s], pol);
+        tma_load_2d_hint(st + TS_BOX, &map_hi, x + 64, y, &tma_full[s], pol);
+        tma_load_2d_hint(st + 2 * TS_BOX, &map_lo, x, y, &tma_full[s], pol);
+        tma_load_2d_hint(st + 3 * TS_BOX, &map_lo, x + 64, y, &tma_full[s], pol);
+        bulk_load(st + 4 * TS_BOX, p.wimg + (size_t)cb * 2 * TS_BTILE, 2 * TS_BTILE,
+                  &tma_full[s]);
+        bulk_load(st + 4 * TS_BOX + 2 * TS_BTILE, p.vimg + (size_t)ab * 2 * TS_BTILE,
+                  2 * TS_BTILE, &tma_full[s]);
+        issued_upto = it + 1;
+      }
+      for (int it = issued_upto - S > 0 ? issued_upto - S : 0; it < issued_upto; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        long long t0 = clock64();
+        while (!mbar_try_wait(&tma_full[s], ph) && clock64() - t0 < M3_DRAIN_BUDGET) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc_t = idesc_bf16_f32(TS_BM, 2 * TS_NPAD);
+      const uint32_t idesc_p = idesc_t | (1u << 15);  // A MN-major (rows c)
+      bool ok = true;
+      for (int it = 0; it < nsteps; ++it) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        const int ci = it / nta, t = it % nta, pb = ci & 1;
+        // P buffer pb was last used by column block ci - 2
+        if (t == 0 && ci >= 2 &&
+            !m3_wait(&p_empty[pb], (uint32_t)((ci >> 1) - 1) & 1u, abort_flag, p.wait_budget)) {
+          ok = false;
+          break;
+        }
+        if (!m3_wait(&tma_full[s], ph, abort_flag, p.wait_budget)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t xh = smem_u32(smem + (size_t)s * TS_STAGE);
+        const uint32_t xl = xh + 2 * TS_BOX;
+        const uint32_t wi = xh + 4 * TS_BOX;
+        const uint32_t vi = wi + 2 * TS_BTILE;
+        const uint32_t acc_t = tmem + (uint32_t)(t * 2 * TS_NPAD);
+        const uint32_t acc_p = tmem + (uint32_t)(TS_TA * 2 * TS_NPAD + pb * 2 * TS_NPAD);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {  // T: K = c, 16 columns (32 B) per slice
+            const uint64_t db = desc_sw128_kmajor(wi + h * TS_BTILE + kk * 32u);
+            const uint32_t first = (ci == 0 && h == 0 && kk == 0) ? 0u : 1u;
+            mma_bf16(acc_t, desc_sw128_kmajor(xh + h * TS_BOX + kk * 32u), db, idesc_t, first);
+            mma_bf16(acc_t, desc_sw128_kmajor(xl + h * TS_BOX + kk * 32u), db, idesc_t, 1u);
+          }
+#pragma unroll
+        for (int kh = 0; kh < 2; ++kh)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {  // P: K = a, 16 rows (2 KB) per slice
+            const uint32_t off = (uint32_t)(kh * 4 + kk) * 2048u;
+            const uint64_t db = desc_sw128_kmajor(vi + kh * TS_BTILE + kk * 32u);
+            const uint32_t first = (t == 0 && kh == 0 && kk == 0) ? 0u : 1u;
+            mma_bf16(acc_p, desc_sw128_mnmajor(xh + off, TS_BOX), db, idesc_p, first);
+            mma_bf16(acc_p, desc_sw128_mnmajor(xl + off, TS_BOX), db, idesc_p, 1u);
+          }
+        mma_commit(&empty[s]);
+        if (t == nta - 1) mma_commit(&p_full[pb]);
+      }
+      if (ok) mma_commit(t_full);
+      if (!ok) {
+        *abort_flag = 1;
+        atomicOr(p.status, DS_TIMEOUT);
+      }
+      mma_commit(mma_done);
+      long long t0 = clock64();
+      while (!mbar_try_wait(mma_done, 0) && clock64() - t0 < M3_DRAIN_BUDGET) {
+      }
+    }
+  } else if (nsteps > 0) {
+    const int q = warp & 3;  // TMEM lane quadrant of this warp
+    const uint32_t lanes = (uint32_t)(q * 32) << 16;
+    bool ok = true;
+    for (int ci = 0; ci < nc; ++ci) {
+      const int pb = ci & 1;
+      int w_ok = 1;
+      if (lane == 0)
+        w_ok = m3_wait(&p_full[pb], (uint32_t)(ci >> 1) & 1u, abort_flag, p.wait_budget) ? 1 : 0;
+      w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+      if (!w_ok) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t c = (int64_t)(cb0 + ci) * 128 + q * 32 + lane;
+      ts_flush(tmem + lanes + (uint32_t)(TS_TA * 2 * TS_NPAD + pb * 2 * TS_NPAD), c, p.C, p.R,
+               p.P);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&p_empty[pb]);
+    }
+    if (ok) {
+      int w_ok = 1;
+      if (lane == 0) w_ok = m3_wait(t_full, 0, abort_flag, p.wait_budget) ? 1 : 0;
+      w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+      ok = w_ok != 0;
+    }
+    if (ok) {
+      tc_fence_after();
+      for (int t = 0; t < nta; ++t) {
+        const int64_t a = (int64_t)(ab0 + t) * TS_BM + q * 32 + lane;
+        ts_flush(tmem + lanes + (uint32_t)(t * 2 * TS_NPAD), a, p.A, p.R, p.T);
+      }
+    } else if (lane == 0) {
+      atomicOr(p.status, DS_TIMEOUT);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TS_TMEM_COLS);
+  }
+}
+
+int encode_map_2d(CUtensorMap* map, const __nv_bfloat16* base, int64_t rows, int64_t cols) {
+  EncodeTiledFn3 enc = encode_fn();
+  if (!enc) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (((uintptr_t)base & 15) || (cols * 2) % 16)
+    return fail(TSR_E_INVALID_ARG, "TMA operand misaligned");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(cols * 2)};
+  cuuint32_t box[2] = {64, (cuuint32_t)TS_BM};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(TSR_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TSR_OK;
+}
+
 size_t m3_smem(const Dense3& d, int mode, int stages) {
   const int L = mode == 2 ? (int)d.J : (int)d.K;
   return 1024 + (size_t)stages * 2 * M3_A_TILE + (size_t)ceil_div(L, M3_BK) * 2 * d.n_pad * 128 +
@@ -551,6 +852,8 @@ size_t m3_smem(const Dense3& d, int mode, int stages) {
 
 void init_mttkrp3_attributes() {
   cudaFuncSetAttribute(mttkrp3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kM3MaxSmem);
+  cudaFuncSetAttribute(twosided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)TS_SMEM);
 }
 
 bool dense3_supported(int ndim, const int64_t* shape, int R) {
@@ -584,8 +887,8 @@ int launch_split_bf16(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, _
 }
 
 int launch_bimage(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t L, int R, int n_pad,
-                  uint8_t* img) {
-  const int chunks = (int)(bimage_bytes(L, n_pad) / 16);
+                  uint8_t* img, int64_t L_img) {
+  const int chunks = (int)(bimage_bytes(std::max(L, L_img), n_pad) / 16);
   bimage_kernel<<<(unsigned)ceil_div(chunks, 256), 256, 0, s>>>(U, (int)L, R, n_pad,
                                                                reinterpret_cast<uint4*>(img),
                                                                chunks);
@@ -643,6 +946,42 @@ int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, cons
   dim3 grid((unsigned)plan.splits, (unsigned)ceil_div(q.rows, M3_BM));
   if (grid.y > 65535) return fail(TSR_E_UNSUPPORTED, "MTTKRP grid too large");
   TSR_CUDA(launch_pdl(mttkrp3_kernel, grid, dim3(M3_THREADS), smem, s, mh, ml, q));
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
+
+bool twosided_supported(int64_t A, int64_t C, int R) {
+  if (R < 1 || R > TS_NPAD || A < 1 || C < 8 || C % 8 != 0) return false;
+  if (A >= INT32_MAX || C >= INT32_MAX) return false;
+  return ceil_div(ceil_div(A, TS_BM), TS_TA) <= 65535;
+}
+
+int64_t twosided_pad(int64_t L) { return ceil_div(L, 128) * 128; }
+
+int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a) {
+  if (!twosided_supported(a.A, a.C, a.R))
+    return fail(TSR_E_UNSUPPORTED, "two-sided contraction: unsupported sizes");
+  CUtensorMap mh, ml;
+  TSR_TRY(encode_map_2d(&mh, a.hi, a.A, a.C));
+  TSR_TRY(encode_map_2d(&ml, a.lo, a.A, a.C));
+  TSParams q;
+  q.A = a.A;
+  q.C = a.C;
+  q.R = a.R;
+  q.nab = (int)ceil_div(a.A, TS_BM);
+  q.ncb = (int)ceil_div(a.C, 128);
+  const int nag = (int)ceil_div(q.nab, TS_TA);
+  const int want = std::max(1, std::min(q.ncb, ctx->sm_count / nag));
+  q.cb_per_split = (int)ceil_div(q.ncb, want);
+  const int splits = (int)ceil_div(q.ncb, q.cb_per_split);
+  q.wimg = a.wimg;
+  q.vimg = a.vimg;
+  q.T = a.T;
+  q.P = a.P;
+  q.status = ctx->d_status;
+  q.wait_budget = ctx->wait_budget;
+  twosided_kernel<<<dim3((unsigned)splits, (unsigned)nag), TS_THREADS, TS_SMEM, s>>>(mh, ml, q);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;

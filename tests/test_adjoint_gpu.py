@@ -97,6 +97,24 @@ def test_loss_grad_vs_cpu_vjp(c5_reference, precision):
         assert rel_err(grads[n], grads_ref[n]) <= 1e-5, (n, rel_err(grads[n], grads_ref[n]))
 
 
+# BF16x3 routes of the loss/gradient on 4+ mode tensors (trailing-two-modes
+# view A x J x K, C = J K): the two-sided contraction (R <= 32, C % 8 == 0)
+# with ragged A and C blocks (128), R % 4 != 0, a five-mode tensor and K % 8
+# != 0; the three-pass single-layout view (32 < R <= 64); the per-mode path.
+@pytest.mark.parametrize("shape,R", [((10, 9, 8, 16), 7), ((5, 6, 24, 40), 12),
+                                     ((3, 4, 5, 6, 16), 8), ((7, 6, 10, 12), 5),
+                                     ((6, 5, 8, 16), 40), ((9, 7, 5, 3), 6)])
+def test_loss_grad_routes_bf16x3(orc, shape, R):
+    rng = np.random.default_rng(sum(shape) + R)
+    X = rng.standard_normal(shape).astype(np.float32)
+    fs = [rng.standard_normal((n, R)).astype(np.float32) for n in shape]
+    loss_ref, grads_ref = orc.cp_loss_grad_vjp(X, fs, C5_REG)
+    loss, grads = tb.cp_loss_grad(X, fs, C5_REG, "bf16x3")
+    assert abs(loss - loss_ref) <= 1e-6 * abs(loss_ref), (loss, loss_ref)
+    for n in range(len(shape)):
+        assert rel_err(grads[n], grads_ref[n]) <= 1e-5, (n, rel_err(grads[n], grads_ref[n]))
+
+
 def test_vjp_path_matches_gram_form(c5_reference):
     """Residual G = 2(Xhat - X) on the GPU, then the reconstruction adjoint
     (tenrso-ad's rule) on G, plus 2 reg U: the recompute form of the same
