@@ -178,12 +178,10 @@ __device__ __forceinline__ double sym_at(const double* g, int R, int a, int c) {
 // <M, U> (= <X, Xhat>) into scal[1]. Shared (FP64): H (R x R), M (rows x R),
 // and the per-group partial sums: `groups` threads share one element of M and
 // each sums a strided subset of the splits with 8 loads in flight.
-__global__ void __launch_bounds__(256)
-gram_grad_kernel(const double* __restrict__ grams, int ndim, int mode,
-                 const float* __restrict__ partials, int splits, int64_t rows, int R,
-                 int rows_per_cta, const float* __restrict__ U, double reg,
-                 float* __restrict__ out, double* scal) {
-  extern __shared__ double sh[];
+__device__ __forceinline__ void gram_grad_block(
+    const double* __restrict__ grams, int ndim, int mode, const float* __restrict__ partials,
+    int splits, int64_t rows, int R, int rows_per_cta, const float* __restrict__ U, double reg,
+    float* __restrict__ out, double* scal, int64_t blk, double* sh) {
   const int RR = R * R;
   double* H = sh;
   double* Ms = sh + RR;
@@ -194,7 +192,7 @@ gram_grad_kernel(const double* __restrict__ grams, int ndim, int mode,
       if (m != mode) h *= sym_at(grams + (int64_t)m * RR, R, a, c);
     H[e] = h;
   }
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+  const int64_t r0 = blk * rows_per_cta;
   const int nr = (int)(rows - r0 < rows_per_cta ? rows - r0 : rows_per_cta);
   const int64_t pstride = rows * R;
   const int ne = nr * R;
@@ -244,9 +242,20 @@ gram_grad_kernel(const double* __restrict__ grams, int ndim, int mode,
   }
 }
 
-// loss = ||X||^2 - 2 <X, Xhat> + sum_{r,s} prod_n Gram_n[r, s] + reg sum_n tr(Gram_n)
-__global__ void gram_loss_kernel(const double* __restrict__ grams, int ndim, int R, double reg,
-                                 double* scal) {
+__global__ void __launch_bounds__(256)
+gram_grad_kernel(const double* __restrict__ grams, int ndim, int mode,
+                 const float* __restrict__ partials, int splits, int64_t rows, int R,
+                 int rows_per_cta, const float* __restrict__ U, double reg,
+                 float* __restrict__ out, double* scal) {
+  extern __shared__ double sh[];
+  gram_grad_block(grams, ndim, mode, partials, splits, rows, R, rows_per_cta, U, reg, out, scal,
+                  blockIdx.x, sh);
+}
+
+// sum_{r,s} prod_n Gram_n[r, s] + reg sum_n tr(Gram_n) over one CTA of
+// `blockDim.x` threads (a multiple of 32), valid in thread 0
+__device__ __forceinline__ double gram_loss_part(const double* __restrict__ grams, int ndim, int R,
+                                                 double reg) {
   const int RR = R * R;
   double s = 0.0;
   for (int e = threadIdx.x; e < RR; e += blockDim.x) {
@@ -263,10 +272,39 @@ __global__ void gram_loss_kernel(const double* __restrict__ grams, int ndim, int
   __shared__ double ws[32];
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
   __syncthreads();
-  if (threadIdx.x != 0) return;
   double t = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
-  scal[2] = scal[0] - 2.0 * scal[1] + t;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+  return t;
+}
+
+// The Grams of every mode in one launch (pre-zeroed): block b is block
+// b - cta0[m] of mode m, rpc[m] rows each.
+struct GramAll {
+  const float* U[kMaxModes];
+  int64_t rows[kMaxModes];
+  int64_t rpc[kMaxModes];
+  int cta0[kMaxModes + 1];
+  int ndim, R;
+  double* grams;
+};
+
+template <int RB>
+__global__ void __launch_bounds__(256) gram_all_kernel(const __grid_constant__ GramAll g) {
+  __shared__ double Us[kGramChunk * 16 * RB];
+  const int b = blockIdx.x;
+  int m = 0;
+  while (m + 1 < g.ndim && b >= g.cta0[m + 1]) ++m;
+  const int64_t r0 = (int64_t)(b - g.cta0[m]) * g.rpc[m];
+  const int64_t r1 = g.rows[m] < r0 + g.rpc[m] ? g.rows[m] : r0 + g.rpc[m];
+  gram_rows_accumulate<RB>(g.U[m], r0, r1, g.R, g.grams + (int64_t)m * g.R * g.R, Us);
+}
+
+// loss = ||X||^2 - 2 <X, Xhat> + sum_{r,s} prod_n Gram_n[r, s] + reg sum_n tr(Gram_n)
+__global__ void gram_loss_kernel(const double* __restrict__ grams, int ndim, int R, double reg,
+                                 double* scal) {
+  const double t = gram_loss_part(grams, ndim, R, reg);
+  if (threadIdx.x == 0) scal[2] = scal[0] - 2.0 * scal[1] + t;
 }
 
 // MTTKRPs from a partial contraction. A side holds S (rows a over nlead
@@ -298,39 +336,133 @@ struct TContract {
   float* out;
 };
 
+// Thread (g, r)'s share of M_m[i, r]: groups g < groups split the side's
+// other indices (FP64).
+__device__ __forceinline__ double t_contract_part(const TSideC& sd, int m, int i, int R, int g,
+                                                  int groups, int r) {
+  double s = 0.0;
+  if (g >= groups) return s;
+  if (sd.nlead == 2) {
+    // the other mode's index is the loop index: four independent loads per step
+    const int o = 1 - m;
+    const int cnt = sd.size[o], so = sd.stride[o];
+    const float* Sp = sd.S + (int64_t)i * sd.stride[m] * R + r;
+    const float* Uo = sd.U[o] + r;
+    int q = g;
+    for (; q + 3 * groups < cnt; q += 4 * groups) {
+      float sv[4], wv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        sv[u] = __ldg(Sp + (int64_t)(q + u * groups) * so * R);
+        wv[u] = __ldg(Uo + (int64_t)(q + u * groups) * R);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) s += (double)sv[u] * (double)wv[u];
+    }
+    for (; q < cnt; q += groups)
+      s += (double)__ldg(Sp + (int64_t)q * so * R) * (double)__ldg(Uo + (int64_t)q * R);
+    return s;
+  }
+  const int count = sd.arows / sd.size[m];
+  for (int q = g; q < count; q += groups) {
+    int rem = q, a = i * sd.stride[m];
+    double w = 1.0;
+    for (int p = sd.nlead - 1; p >= 0; --p) {
+      if (p == m) continue;
+      const int ip = rem % sd.size[p];
+      rem /= sd.size[p];
+      a += ip * sd.stride[p];
+      w *= (double)__ldg(sd.U[p] + (int64_t)ip * R + r);
+    }
+    s += (double)__ldg(sd.S + (int64_t)a * R + r) * w;
+  }
+  return s;
+}
+
 __global__ void __launch_bounds__(256) t_contract_kernel(const __grid_constant__ TContract c) {
   __shared__ double part[256];
   const int b = blockIdx.x;
   int n = 0;
   while (n + 1 < c.nmodes && b >= c.row0[n + 1]) ++n;
-  const TSideC& sd = c.side[c.side_of[n]];
-  const int m = c.pos[n];
-  const int i = b - c.row0[n];
   const int R = c.R;
   const int groups = blockDim.x / R;
-  const int g = threadIdx.x / R, r = threadIdx.x % R;
-  double s = 0.0;
-  if (g < groups) {
-    const int count = sd.arows / sd.size[m];
-    for (int q = g; q < count; q += groups) {
-      int rem = q, a = i * sd.stride[m];
-      double w = 1.0;
-      for (int p = sd.nlead - 1; p >= 0; --p) {
-        if (p == m) continue;
-        const int ip = rem % sd.size[p];
-        rem /= sd.size[p];
-        a += ip * sd.stride[p];
-        w *= (double)__ldg(sd.U[p] + (int64_t)ip * R + r);
-      }
-      s += (double)__ldg(sd.S + (int64_t)a * R + r) * w;
-    }
-  }
-  part[threadIdx.x] = s;
+  part[threadIdx.x] = t_contract_part(c.side[c.side_of[n]], c.pos[n], b - c.row0[n], R,
+                                      threadIdx.x / R, groups, threadIdx.x % R);
   __syncthreads();
   if (threadIdx.x < R) {
     double t = 0.0;
     for (int q = 0; q < groups; ++q) t += part[q * R + threadIdx.x];
     c.out[(int64_t)b * R + threadIdx.x] = (float)t;
+  }
+}
+
+// The same contraction with the gradient row formed in place (R <= 32): block
+// b is row i of mode n; with M_n[i, :] reduced in shared memory,
+//   grad[i, c] = 2 (sum_k U_n[i, k] H_n[k, c] - M_n[i, c] + reg U_n[i, c]),
+// H_n = *_{m != n} Gram_m formed by the block (FP64, the Grams stay in L1).
+// Mode-0 rows add <M_0, U_0> (= <X, Xhat>) into scal[1]; the extra last
+// block writes the Gram part of the loss into scal[3].
+struct GradArgs {
+  const double* grams;
+  int ndim;
+  double reg;
+  float* G[kMaxModes];
+  double* scal;
+};
+
+__global__ void __launch_bounds__(256)
+t_contract_grad_kernel(const __grid_constant__ TContract c, const __grid_constant__ GradArgs ga) {
+  __shared__ double part[256];
+  __shared__ double H[32 * 32];
+  __shared__ double Mrow[32];
+  const int b = blockIdx.x;
+  const int R = c.R;
+  if (b >= c.row0[c.nmodes]) {
+    const double t = gram_loss_part(ga.grams, ga.ndim, R, ga.reg);
+    if (threadIdx.x == 0) ga.scal[3] = t;
+    return;
+  }
+  int n = 0;
+  while (n + 1 < c.nmodes && b >= c.row0[n + 1]) ++n;
+  const TSideC& sd = c.side[c.side_of[n]];
+  const int m = c.pos[n], i = b - c.row0[n];
+  const int groups = blockDim.x / R;
+  part[threadIdx.x] = t_contract_part(sd, m, i, R, threadIdx.x / R, groups, threadIdx.x % R);
+  const int RR = R * R;
+  for (int e = threadIdx.x; e < RR; e += blockDim.x) {
+    const int a = e / R, cc = e % R;
+    double h = 1.0;
+    for (int q = 0; q < ga.ndim; ++q)
+      if (q != n) h *= sym_at(ga.grams + (int64_t)q * RR, R, a, cc);
+    H[e] = h;
+  }
+  __syncthreads();
+  if (threadIdx.x < R) {
+    double t = 0.0;
+    for (int q = 0; q < groups; ++q) t += part[q * R + threadIdx.x];
+    Mrow[threadIdx.x] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {  // R <= 32: one warp
+    const int cc = threadIdx.x;
+    double ip = 0.0;
+    if (cc < R) {
+      const float* urow = sd.U[m] + (int64_t)i * R;
+      double s0 = 0.0, s1 = 0.0;
+      int k = 0;
+      for (; k + 2 <= R; k += 2) {
+        s0 += (double)__ldg(urow + k) * H[k * R + cc];
+        s1 += (double)__ldg(urow + k + 1) * H[(k + 1) * R + cc];
+      }
+      if (k < R) s0 += (double)__ldg(urow + k) * H[k * R + cc];
+      const double u = (double)__ldg(urow + cc);
+      ga.G[n][(int64_t)i * R + cc] = (float)(2.0 * ((s0 + s1) - Mrow[cc] + ga.reg * u));
+      ip = Mrow[cc] * u;
+    }
+    if (n == 0) {
+      for (int o = 16; o > 0; o >>= 1) ip += __shfl_down_sync(0xffffffffu, ip, o);
+      if (cc == 0) atomicAdd(ga.scal + 1, ip);
+    }
   }
 }
 
@@ -717,9 +849,35 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
   void* gp;
   TSR_TRY(slot_get(ctx, SLOT_GRAMS, sizeof(double) * N * RR, &gp));
   double* grams = (double*)gp;
-  for (int m = 0; m < N; ++m)
-    TSR_TRY(launch_gram(ctx, ctx->stream, d_factors[m], X->shape[m], R, grams + (size_t)m * RR,
-                        true));
+  {
+    // every mode's Gram in one launch
+    TSR_CUDA(cudaMemsetAsync(grams, 0, sizeof(double) * N * RR, ctx->stream));
+    GramAll ga{};
+    ga.ndim = N;
+    ga.R = R;
+    ga.grams = grams;
+    ga.cta0[0] = 0;
+    for (int m = 0; m < N; ++m) {
+      const int64_t rows = X->shape[m];
+      int64_t ctas = std::min<int64_t>(ceil_div(rows, 16), 2 * ctx->sm_count);
+      ga.rpc[m] = ceil_div(rows, ctas);
+      ga.U[m] = d_factors[m];
+      ga.rows[m] = rows;
+      ga.cta0[m + 1] = ga.cta0[m] + (int)ceil_div(rows, ga.rpc[m]);
+    }
+    const unsigned g = (unsigned)ga.cta0[N];
+    switch ((R + 15) / 16) {
+      case 1: gram_all_kernel<1><<<g, 256, 0, ctx->stream>>>(ga); break;
+      case 2: gram_all_kernel<2><<<g, 256, 0, ctx->stream>>>(ga); break;
+      case 3: gram_all_kernel<3><<<g, 256, 0, ctx->stream>>>(ga); break;
+      case 4: gram_all_kernel<4><<<g, 256, 0, ctx->stream>>>(ga); break;
+      case 5: gram_all_kernel<5><<<g, 256, 0, ctx->stream>>>(ga); break;
+      case 6: gram_all_kernel<6><<<g, 256, 0, ctx->stream>>>(ga); break;
+      default: gram_all_kernel<7><<<g, 256, 0, ctx->stream>>>(ga); break;
+    }
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+  }
   TSR_CUDA(cudaMemsetAsync(X->d_scalars + 1, 0, 2 * sizeof(double), ctx->stream));
   auto grad_of = [&](int n, const float* partials, int splits) -> int {
     const int64_t rows = X->shape[n];
@@ -741,8 +899,8 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     gram_loss_kernel<<<1, 256, 0, ctx->stream>>>(grams, N, R, reg, X->d_scalars);
     ctx->launches++;
     TSR_CUDA(cudaGetLastError());
-    TSR_TRY(check_device_status(ctx));
     if (loss) {
+      TSR_TRY(check_device_status(ctx));
       TSR_CUDA(cudaMemcpyAsync(loss, X->d_scalars + 2, sizeof(double), cudaMemcpyDeviceToHost,
                                ctx->stream));
       TSR_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -755,25 +913,28 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     // mode's MTTKRP from T (modes 0..N-3) or P (modes N-2, N-1)
     const int64_t A = X->d3.I, C = X->d3.J * X->d3.K;
     const int64_t Ap = twosided_pad(A), Cp = twosided_pad(C);
-    void *kp, *kq, *wp, *tp, *mp, *ip;
-    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * A * R, &kp));
-    TSR_TRY(slot_get(ctx, SLOT_MISC3, sizeof(float) * A * R, &kq));
-    TSR_TRY(slot_get(ctx, SLOT_PARTIALS, sizeof(float) * C * R, &wp));
-    const float* kr = d_factors[0];
-    int64_t krows = X->shape[0];
-    float* bufs[2] = {(float*)kp, (float*)kq};
-    for (int p = 1; p < N - 2; ++p) {
-      float* dst = bufs[p & 1];
-      TSR_TRY(launch_khatri_rao(ctx, kr, krows, d_factors[p], X->shape[p], R, dst));
-      kr = dst;
-      krows *= X->shape[p];
-    }
-    TSR_TRY(launch_khatri_rao(ctx, d_factors[N - 2], X->d3.J, d_factors[N - 1], X->d3.K, R,
-                              (float*)wp));
+    void *tp, *ip;
+    // B images of V = KR(leading factors) and W = KR(trailing two), rows
+    // formed on the fly
     const size_t vb = bimage_bytes(Ap, 32), wb = bimage_bytes(Cp, 32);
     TSR_TRY(slot_get(ctx, SLOT_D3_IMG, vb + wb, &ip));
-    TSR_TRY(launch_bimage(ctx, ctx->stream, kr, A, R, 32, (uint8_t*)ip, Ap));
-    TSR_TRY(launch_bimage(ctx, ctx->stream, (const float*)wp, C, R, 32, (uint8_t*)ip + vb, Cp));
+    KRImages ki{};
+    ki.n = 2;
+    ki.R = R;
+    ki.n_pad = 32;
+    for (int w = 0; w < 2; ++w) {
+      KRImage& im = ki.im[w];
+      const int m0 = w == 0 ? 0 : N - 2, m1 = w == 0 ? N - 2 : N;
+      im.nf = m1 - m0;
+      for (int f = 0; f < im.nf; ++f) {
+        im.U[f] = d_factors[m0 + f];
+        im.size[f] = X->shape[m0 + f];
+      }
+      im.L = w == 0 ? A : C;
+      im.chunks = (int)((w == 0 ? vb : wb) / 16);
+      im.img = (uint8_t*)ip + (w == 0 ? 0 : vb);
+    }
+    TSR_TRY(launch_kr_images(ctx, ctx->stream, ki));
     TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * (A + C) * R, &tp));
     TSR_CUDA(cudaMemsetAsync(tp, 0, sizeof(float) * (A + C) * R, ctx->stream));
     TwoSided ts;
@@ -789,7 +950,6 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     TSR_TRY(launch_twosided(ctx, ctx->stream, ts));
     int total_rows = 0;
     for (int p = 0; p < N; ++p) total_rows += (int)X->shape[p];
-    TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(float) * total_rows * R, &mp));
     TContract c{};
     set_side(c, 0, ts.T, X->shape, 0, N - 2, d_factors);
     set_side(c, 1, ts.P, X->shape, N - 2, N, d_factors);
@@ -801,13 +961,24 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
       c.pos[p] = p < N - 2 ? p : p - (N - 2);
       c.row0[p + 1] = c.row0[p] + (int)X->shape[p];
     }
-    c.out = (float*)mp;
-    t_contract_kernel<<<(unsigned)total_rows, 256, 0, ctx->stream>>>(c);
+    // every mode's MTTKRP and gradient rows, and the Gram part of the loss
+    GradArgs g{};
+    g.grams = grams;
+    g.ndim = N;
+    g.reg = reg;
+    g.scal = X->d_scalars;
+    for (int m = 0; m < N; ++m) g.G[m] = d_grads[m];
+    t_contract_grad_kernel<<<(unsigned)total_rows + 1, 256, 0, ctx->stream>>>(c, g);
     ctx->launches++;
     TSR_CUDA(cudaGetLastError());
-    for (int m = 0; m < N; ++m)
-      TSR_TRY(grad_of(m, (const float*)mp + (int64_t)c.row0[m] * R, 1));
-    return finish();
+    if (loss) {
+      TSR_TRY(check_device_status(ctx));
+      double sc[4];
+      TSR_CUDA(cudaMemcpyAsync(sc, X->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      *loss = sc[0] - 2.0 * sc[1] + sc[3];
+    }
+    return TSR_OK;
   }
   if (X->d3_on && X->d3_three && R <= 64) {
     // three single-layout passes over X's bf16 halves instead of one MTTKRP
@@ -889,29 +1060,9 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     float* partials;
     int splits;
     TSR_TRY(run_mttkrp_partials(ctx, X->ops[n], ft, R, X->precision, &partials, &splits));
-    const int64_t rows = X->shape[n];
-    const int rpc =
-        (int)std::max<int64_t>(1, std::min<int64_t>(16, ceil_div(rows, 2 * ctx->sm_count)));
-    const int full = rpc * R;
-    const int groups = full >= 256 ? 1 : 256 / full;
-    const size_t smem = sizeof(double) * ((size_t)RR + full + (size_t)groups * full);
-    if (smem > 200 * 1024)
-      return fail(TSR_E_UNSUPPORTED, "rank %d too large for the gradient kernel", R);
-    gram_grad_kernel<<<(unsigned)ceil_div(rows, rpc), 256, smem, ctx->stream>>>(
-        grams, N, n, partials, splits, rows, R, rpc, d_factors[n], reg, d_grads[n],
-        X->d_scalars);
-    ctx->launches++;
-    TSR_CUDA(cudaGetLastError());
+    TSR_TRY(grad_of(n, partials, splits));
   }
-  gram_loss_kernel<<<1, 256, 0, ctx->stream>>>(grams, N, R, reg, X->d_scalars);
-  ctx->launches++;
-  TSR_CUDA(cudaGetLastError());
-  if (loss) {
-    TSR_CUDA(cudaMemcpyAsync(loss, X->d_scalars + 2, sizeof(double), cudaMemcpyDeviceToHost,
-                             ctx->stream));
-    TSR_CUDA(cudaStreamSynchronize(ctx->stream));
-  }
-  return TSR_OK;
+  return finish();
 }
 
 }  // extern "C"

@@ -17,54 +17,16 @@ namespace tsr {
 
 namespace {
 
-// Upper triangle of U^T U accumulated into `gram` (pre-zeroed) with one FP64
-// atomic per entry per CTA. Thread (ty, tx) of a 16 x 16 grid owns entries
-// (ty + 16a, tx + 16b); rows are staged through shared memory in chunks, so a
-// row costs 2*RB shared loads for RB*RB FMAs. Products of fp32 values are
-// exact in FP64.
+// Upper triangle of U^T U accumulated into `gram` (pre-zeroed); the body is
+// gram_rows_accumulate (als.cuh), rows_per_cta rows per CTA.
 template <int RB>
 __global__ void __launch_bounds__(256)
 gram_kernel(const float* __restrict__ U, int64_t rows, int R, int64_t rows_per_cta,
             double* __restrict__ gram) {
-  constexpr int CH = 32;
-  __shared__ double Us[CH * 16 * RB];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[RB][RB];
-#pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
-#pragma unroll
-    for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = 0.0;
+  __shared__ double Us[kGramChunk * 16 * RB];
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
   const int64_t r1 = rows < r0 + rows_per_cta ? rows : r0 + rows_per_cta;
-  const int LD = 16 * RB;
-  for (int64_t c0 = r0; c0 < r1; c0 += CH) {
-    const int nr = (int)(r1 - c0 < CH ? r1 - c0 : CH);
-    __syncthreads();
-#pragma unroll 4
-    for (int k = threadIdx.x; k < nr * LD; k += 256) {
-      const int i = k / LD, c = k % LD;
-      Us[k] = c < R ? (double)__ldg(U + (c0 + i) * R + c) : 0.0;
-    }
-    __syncthreads();
-    for (int i = 0; i < nr; ++i) {
-      double x[RB], y[RB];
-#pragma unroll
-      for (int ai = 0; ai < RB; ++ai) x[ai] = Us[i * LD + ty + 16 * ai];
-#pragma unroll
-      for (int bj = 0; bj < RB; ++bj) y[bj] = Us[i * LD + tx + 16 * bj];
-#pragma unroll
-      for (int ai = 0; ai < RB; ++ai)
-#pragma unroll
-        for (int bj = 0; bj < RB; ++bj) acc[ai][bj] += x[ai] * y[bj];
-    }
-  }
-#pragma unroll
-  for (int ai = 0; ai < RB; ++ai)
-#pragma unroll
-    for (int bj = 0; bj < RB; ++bj) {
-      const int a = ty + 16 * ai, c = tx + 16 * bj;
-      if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
-    }
+  gram_rows_accumulate<RB>(U, r0, r1, R, gram, Us);
 }
 
 __global__ void norm_sq_kernel(const float* __restrict__ X, int64_t n, double* out) {

@@ -24,6 +24,54 @@ struct AlsState {
   int pad;
 };
 
+// Upper triangle of U[r0:r1]^T U[r0:r1] added into `gram` (row a, column
+// c >= a) with one FP64 atomic per entry per CTA of 256 threads. Thread
+// (ty, tx) of a 16 x 16 grid owns entries (ty + 16a, tx + 16b); rows are
+// staged through shared memory (Us: kGramChunk * 16 * RB doubles) in chunks,
+// so a row costs 2*RB shared loads for RB*RB FMAs. Products of fp32 values
+// are exact in FP64.
+constexpr int kGramChunk = 32;
+template <int RB>
+__device__ __forceinline__ void gram_rows_accumulate(const float* __restrict__ U, int64_t r0,
+                                                     int64_t r1, int R, double* __restrict__ gram,
+                                                     double* Us) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[RB][RB];
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) acc[ai][bj] = 0.0;
+  const int LD = 16 * RB;
+  for (int64_t c0 = r0; c0 < r1; c0 += kGramChunk) {
+    const int nr = (int)(r1 - c0 < kGramChunk ? r1 - c0 : kGramChunk);
+    __syncthreads();
+#pragma unroll 4
+    for (int k = threadIdx.x; k < nr * LD; k += 256) {
+      const int i = k / LD, c = k % LD;
+      Us[k] = c < R ? (double)__ldg(U + (c0 + i) * R + c) : 0.0;
+    }
+    __syncthreads();
+    for (int i = 0; i < nr; ++i) {
+      double x[RB], y[RB];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai) x[ai] = Us[i * LD + ty + 16 * ai];
+#pragma unroll
+      for (int bj = 0; bj < RB; ++bj) y[bj] = Us[i * LD + tx + 16 * bj];
+#pragma unroll
+      for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+        for (int bj = 0; bj < RB; ++bj) acc[ai][bj] += x[ai] * y[bj];
+    }
+  }
+#pragma unroll
+  for (int ai = 0; ai < RB; ++ai)
+#pragma unroll
+    for (int bj = 0; bj < RB; ++bj) {
+      const int a = ty + 16 * ai, c = tx + 16 * bj;
+      if (a < R && c < R && c >= a) atomicAdd(gram + a * R + c, acc[ai][bj]);
+    }
+}
+
 struct AlsBuffers {
   double* grams;    // [N][R][R]   U_m^T U_m
   double* hadam;    // [N][R][R]   Hadamard of the other Grams (G_n)

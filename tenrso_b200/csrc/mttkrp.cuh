@@ -80,6 +80,25 @@ struct TwoSided {
   float* T;
   float* P;
 };
+// B images (n_pad rows of hi halves, n_pad of lo halves per 64-row block) of
+// Khatri-Rao products, built on the fly: row k of image w is the product of
+// im[w].U[f][k_f, :] over the row-major multi-index (k_0, ..., k_{nf-1}) of k
+// over the factors' row counts; rows from L on are zero. chunks = image
+// bytes / 16 (bimage_bytes of the padded row count).
+struct KRImage {
+  int nf;
+  const float* U[kMaxModes];
+  int size[kMaxModes];
+  int L;
+  int chunks;
+  uint8_t* img;
+};
+struct KRImages {
+  KRImage im[2];
+  int n;  // images in use (1 or 2)
+  int R, n_pad;
+};
+int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a);
 bool twosided_supported(int64_t A, int64_t C, int R);
 int64_t twosided_pad(int64_t L);
 int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a);

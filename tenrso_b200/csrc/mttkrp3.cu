@@ -470,6 +470,52 @@ __global__ void bimage_kernel(const float* __restrict__ U, int L, int R, int n_p
   img[e] = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
+// B images of Khatri-Rao products, the layout of bimage_kernel, up to two
+// images per launch: row k of a product is the row-major multi-index over its
+// factors' rows, each entry the fp32 product of the factors' entries.
+__global__ void kr_images_kernel(const __grid_constant__ KRImages a) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  int w = 0;
+  if (e >= a.im[0].chunks) {
+    e -= a.im[0].chunks;
+    w = 1;
+    if (a.n < 2 || e >= a.im[1].chunks) return;
+  }
+  const KRImage& im = a.im[w];
+  const int pos = e & 7;
+  const int rows = 2 * a.n_pad;
+  const int row = (e >> 3) % rows;
+  const int kb = (e >> 3) / rows;
+  const int c = pos ^ (row & 7);
+  const int n = row < a.n_pad ? row : row - a.n_pad;
+  const bool want_lo = row >= a.n_pad;
+  uint32_t wv[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float v[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = kb * 64 + c * 8 + 2 * q + h;
+      float x = 0.f;
+      if (n < a.R && k < im.L) {
+        x = 1.f;
+        int rem = k;
+        for (int f = im.nf - 1; f >= 0; --f) {
+          const int sz = im.size[f];
+          const int nxt = rem / sz;
+          x *= __ldg(im.U[f] + (int64_t)(rem - nxt * sz) * a.R + n);
+          rem = nxt;
+        }
+      }
+      const float hx = __bfloat162float(__float2bfloat16_rn(x));
+      v[h] = want_lo ? x - hx : hx;
+    }
+    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[0], v[1]);
+    wv[q] = *reinterpret_cast<const uint32_t*>(&b2);
+  }
+  reinterpret_cast<uint4*>(im.img)[e] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point.
 typedef CUresult (*EncodeTiledFn3)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -958,6 +1004,24 @@ bool twosided_supported(int64_t A, int64_t C, int R) {
 }
 
 int64_t twosided_pad(int64_t L) { return ceil_div(L, 128) * 128; }
+
+int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a) {
+  if (a.n < 1 || a.n > 2) return fail(TSR_E_INVALID_ARG, "one or two images per launch");
+  int64_t total = 0;
+  for (int w = 0; w < a.n; ++w) {
+    if (a.im[w].nf < 1 || a.im[w].nf > kMaxModes)
+      return fail(TSR_E_INVALID_ARG, "Khatri-Rao image of %d factors", a.im[w].nf);
+    // row indices in 32 bits: the padded row count below 2^31
+    if ((int64_t)a.im[w].chunks * 16 / (2 * a.n_pad * 2) >= INT32_MAX)
+      return fail(TSR_E_UNSUPPORTED, "Khatri-Rao image too large");
+    total += a.im[w].chunks;
+  }
+  if (total <= 0) return TSR_OK;
+  kr_images_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, s>>>(a);
+  ctx->launches++;
+  TSR_CUDA(cudaGetLastError());
+  return TSR_OK;
+}
 
 int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a) {
   if (!twosided_supported(a.A, a.C, a.R))
