@@ -476,8 +476,10 @@ def run_adjoint(tb, torch, ctx, stream, args, world, dist, rank):
     fptr = [f.data_ptr() for f in dF]
     gptr = [g.data_ptr() for g in dGr]
     steps = max(5, args.steps)
+    # algorithmic bytes: fp32, one MTTKRP read of X per mode (4 x 4 B per
+    # element); bf16x3, one two-sided read of X's bf16 halves (4 B per element)
     out = {"workload": "CP loss+gradient 128x96x64x48, rank 32, reg 1e-3",
-           "bytes_alg_per_eval": 4 * 4 * X.size}
+           "bytes_alg_per_eval": {"fp32": 4 * 4 * X.size, "bf16x3": 4 * X.size}}
 
     def timed(fn):
         for _ in range(max(3, args.warmup)):
@@ -505,7 +507,7 @@ def run_adjoint(tb, torch, ctx, stream, args, world, dist, rank):
         out[f"gram_form_{prec}"] = {
             "evals_per_s": world * 1e3 / ms, "ms_per_eval": ms, "loss": loss,
             "launches_per_eval": launches,
-            "achieved_gbs": out["bytes_alg_per_eval"] / (ms * 1e-3) / 1e9}
+            "achieved_gbs": out["bytes_alg_per_eval"][prec] / (ms * 1e-3) / 1e9}
     dG = torch.empty_like(dX)
 
     def recompute():
