@@ -192,6 +192,26 @@ __device__ bool solve_mode(const InstSmem& s, const float* M, int rows, int R, i
   return true;
 }
 
+// acc[p][r] += x[p] * W[r] for the four k of x (W: one shared-memory factor
+// row, Rp floats)
+template <int RQ>
+__device__ __forceinline__ void fma_row4(float (&acc)[4][4 * RQ], const float4 x,
+                                         const float* W) {
+  const float4* w4 = reinterpret_cast<const float4*>(W);
+#pragma unroll
+  for (int rq = 0; rq < RQ; ++rq) {
+    const float4 b = w4[rq];
+    const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      acc[0][4 * rq + h] = fmaf(x.x, bb[h], acc[0][4 * rq + h]);
+      acc[1][4 * rq + h] = fmaf(x.y, bb[h], acc[1][4 * rq + h]);
+      acc[2][4 * rq + h] = fmaf(x.z, bb[h], acc[2][4 * rq + h]);
+      acc[3][4 * rq + h] = fmaf(x.w, bb[h], acc[3][4 * rq + h]);
+    }
+  }
+}
+
 // pass 1: M[i, r] += sum_k (sum_j X[i, j, k] B[j, r]) C[k, r]
 template <int NT, int RQ>
 __device__ void pass_v(const float4* __restrict__ X4, int n0, int n1, int nkq, const float* B,
@@ -209,23 +229,16 @@ __device__ void pass_v(const float4* __restrict__ X4, int n0, int n1, int nkq, c
 #pragma unroll
       for (int r = 0; r < Rp; ++r) acc[p][r] = 0.f;
     const float4* xp = X4 + (size_t)i * n1 * nkq + kq;
-#pragma unroll 2
-    for (int j = g; j < n1; j += split) {
-      const float4 x = __ldg(xp + (size_t)j * nkq);
-      const float4* b4 = reinterpret_cast<const float4*>(B + j * Rp);
+    // four loads of X in flight per thread, then their FMAs in j order
+    int j = g;
+    for (; j + 3 * split < n1; j += 4 * split) {
+      float4 xs[4];
 #pragma unroll
-      for (int rq = 0; rq < RQ; ++rq) {
-        const float4 b = b4[rq];
-        const float bb[4] = {b.x, b.y, b.z, b.w};
+      for (int u = 0; u < 4; ++u) xs[u] = __ldg(xp + (size_t)(j + u * split) * nkq);
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          acc[0][4 * rq + h] = fmaf(x.x, bb[h], acc[0][4 * rq + h]);
-          acc[1][4 * rq + h] = fmaf(x.y, bb[h], acc[1][4 * rq + h]);
-          acc[2][4 * rq + h] = fmaf(x.z, bb[h], acc[2][4 * rq + h]);
-          acc[3][4 * rq + h] = fmaf(x.w, bb[h], acc[3][4 * rq + h]);
-        }
-      }
+      for (int u = 0; u < 4; ++u) fma_row4<RQ>(acc, xs[u], B + (j + u * split) * Rp);
     }
+    for (; j < n1; j += split) fma_row4<RQ>(acc, __ldg(xp + (size_t)j * nkq), B + j * Rp);
 #pragma unroll
     for (int r = 0; r < Rp; ++r) {
       float v = 0.f;
@@ -255,23 +268,15 @@ __device__ void pass_u(const float4* __restrict__ X4, int n0, int n1, int nkq, c
       for (int r = 0; r < Rp; ++r) acc[p][r] = 0.f;
     const float4* xp = X4 + (size_t)j * nkq + kq;
     const size_t istride = (size_t)n1 * nkq;
-#pragma unroll 2
-    for (int i = g; i < n0; i += split) {
-      const float4 x = __ldg(xp + (size_t)i * istride);
-      const float4* a4 = reinterpret_cast<const float4*>(A + i * Rp);
+    int i = g;
+    for (; i + 3 * split < n0; i += 4 * split) {
+      float4 xs[4];
 #pragma unroll
-      for (int rq = 0; rq < RQ; ++rq) {
-        const float4 av = a4[rq];
-        const float aa[4] = {av.x, av.y, av.z, av.w};
+      for (int u = 0; u < 4; ++u) xs[u] = __ldg(xp + (size_t)(i + u * split) * istride);
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          acc[0][4 * rq + h] = fmaf(x.x, aa[h], acc[0][4 * rq + h]);
-          acc[1][4 * rq + h] = fmaf(x.y, aa[h], acc[1][4 * rq + h]);
-          acc[2][4 * rq + h] = fmaf(x.z, aa[h], acc[2][4 * rq + h]);
-          acc[3][4 * rq + h] = fmaf(x.w, aa[h], acc[3][4 * rq + h]);
-        }
-      }
+      for (int u = 0; u < 4; ++u) fma_row4<RQ>(acc, xs[u], A + (i + u * split) * Rp);
     }
+    for (; i < n0; i += split) fma_row4<RQ>(acc, __ldg(xp + (size_t)i * istride), A + i * Rp);
 #pragma unroll
     for (int r = 0; r < Rp; ++r) {
       float v = 0.f;
