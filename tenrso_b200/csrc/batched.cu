@@ -76,6 +76,7 @@ struct InstSmem {
   float* A;   // n0 x Rp
   float* B;   // n1 x Rp
   float* C;   // n2p x Rp (rows >= n2 are zero)
+  float* Ct;  // Rp x n2p: C transposed, for conflict-free float4 reads of four C rows
   float* M;   // max(n0, n1, n2p) x Rp
   double* GA;  // 16 x 16 each (FP64 Grams)
   double* GB;
@@ -99,14 +100,15 @@ __device__ __forceinline__ InstSmem carve(unsigned char* base, const BatchInst& 
   s.A = f;
   s.B = s.A + in.n0 * Rp;
   s.C = s.B + in.n1 * Rp;
-  s.M = s.C + in.n2p * Rp;
+  s.Ct = s.C + in.n2p * Rp;
+  s.M = s.Ct + in.n2p * Rp;
   return s;
 }
 
 __host__ __device__ inline size_t inst_smem_bytes(int n0, int n1, int n2p, int rq) {
   const int Rp = 4 * rq;
   const int mx = n0 > n1 ? (n0 > n2p ? n0 : n2p) : (n1 > n2p ? n1 : n2p);
-  return sizeof(double) * 1312 + sizeof(float) * (size_t)(n0 + n1 + n2p + mx) * Rp;
+  return sizeof(double) * 1312 + sizeof(float) * (size_t)(n0 + n1 + 2 * n2p + mx) * Rp;
 }
 
 // Block sum of one double per thread (all threads call it).
@@ -212,10 +214,19 @@ __device__ __forceinline__ void fma_row4(float (&acc)[4][4 * RQ], const float4 x
   }
 }
 
+// Ct = C^T (Rp x n2p), the whole CTA; ends with a barrier.
+__device__ __forceinline__ void transpose_c(const InstSmem& s, int n2p, int Rp, int nt) {
+  for (int e = threadIdx.x; e < n2p * Rp; e += nt) {
+    const int k = e / Rp, r = e - k * Rp;
+    s.Ct[r * n2p + k] = s.C[e];
+  }
+  __syncthreads();
+}
+
 // pass 1: M[i, r] += sum_k (sum_j X[i, j, k] B[j, r]) C[k, r]
 template <int NT, int RQ>
 __device__ void pass_v(const float4* __restrict__ X4, int n0, int n1, int nkq, const float* B,
-                       const float* C, float* M, int R) {
+                       const float* Ct, float* M, int R) {
   constexpr int Rp = 4 * RQ;
   const int nq = n0 * nkq;
   const int split = nq >= NT ? 1 : min(n1, NT / nq);
@@ -239,11 +250,16 @@ __device__ void pass_v(const float4* __restrict__ X4, int n0, int n1, int nkq, c
       for (int u = 0; u < 4; ++u) fma_row4<RQ>(acc, xs[u], B + (j + u * split) * Rp);
     }
     for (; j < n1; j += split) fma_row4<RQ>(acc, __ldg(xp + (size_t)j * nkq), B + j * Rp);
+    // C rows 4kq .. 4kq+3 at column r: one float4 of Ct (lanes read
+    // consecutive float4s; the rows of C would all map to one bank)
+    const float4* Ct4 = reinterpret_cast<const float4*>(Ct);
 #pragma unroll
     for (int r = 0; r < Rp; ++r) {
-      float v = 0.f;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) v = fmaf(acc[p][r], C[(4 * kq + p) * Rp + r], v);
+      const float4 c = Ct4[r * nkq + kq];
+      float v = fmaf(acc[0][r], c.x, 0.f);
+      v = fmaf(acc[1][r], c.y, v);
+      v = fmaf(acc[2][r], c.z, v);
+      v = fmaf(acc[3][r], c.w, v);
       if (r < R) atomicAdd(M + i * Rp + r, v);
     }
   }
@@ -253,7 +269,7 @@ __device__ void pass_v(const float4* __restrict__ X4, int n0, int n1, int nkq, c
 // M[j, r] += sum_k U[j, k, r] C[k, r]
 template <int NT, int RQ>
 __device__ void pass_u(const float4* __restrict__ X4, int n0, int n1, int nkq, const float* A,
-                       const float* C, float* M, float* U, int R) {
+                       const float* Ct, float* M, float* U, int R) {
   constexpr int Rp = 4 * RQ;
   const int nq = n1 * nkq;
   const int split = nq >= NT ? 1 : min(n0, NT / nq);
@@ -277,11 +293,14 @@ __device__ void pass_u(const float4* __restrict__ X4, int n0, int n1, int nkq, c
       for (int u = 0; u < 4; ++u) fma_row4<RQ>(acc, xs[u], A + (i + u * split) * Rp);
     }
     for (; i < n0; i += split) fma_row4<RQ>(acc, __ldg(xp + (size_t)i * istride), A + i * Rp);
+    const float4* Ct4 = reinterpret_cast<const float4*>(Ct);
 #pragma unroll
     for (int r = 0; r < Rp; ++r) {
-      float v = 0.f;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) v = fmaf(acc[p][r], C[(4 * kq + p) * Rp + r], v);
+      const float4 c = Ct4[r * nkq + kq];
+      float v = fmaf(acc[0][r], c.x, 0.f);
+      v = fmaf(acc[1][r], c.y, v);
+      v = fmaf(acc[2][r], c.z, v);
+      v = fmaf(acc[3][r], c.w, v);
       if (r < R) atomicAdd(M + j * Rp + r, v);
     }
     // U rows (j, 4kq + p), Rp floats each
@@ -330,6 +349,7 @@ __device__ void run_instance(const BatchArgs& a, int id, unsigned char* smem_raw
     s.C[e] = (r < R && i < n2) ? F[(size_t)(n0 + n1 + i) * R + r] : 0.f;
   }
   __syncthreads();
+  transpose_c(s, n2p, Rp, NT);
   gram16<NT>(s.A, n0, Rp, s.GA);
   gram16<NT>(s.B, n1, Rp, s.GB);
   gram16<NT>(s.C, n2p, Rp, s.GC);
@@ -340,7 +360,7 @@ __device__ void run_instance(const BatchArgs& a, int id, unsigned char* smem_raw
     // ---- mode 0
     for (int e = threadIdx.x; e < n0 * Rp; e += NT) s.M[e] = 0.f;
     __syncthreads();
-    pass_v<NT, RQ>(X4, n0, n1, nkq, s.B, s.C, s.M, R);
+    pass_v<NT, RQ>(X4, n0, n1, nkq, s.B, s.Ct, s.M, R);
     __syncthreads();
     bool ok = solve_mode<NT>(s, s.M, n0, R, Rp, s.GB, s.GC, s.A, s.GA, ridge_eps, &ridge_used);
     // ---- mode 1
@@ -353,7 +373,7 @@ __device__ void run_instance(const BatchArgs& a, int id, unsigned char* smem_raw
         for (int e = threadIdx.x; e < n4; e += NT) u4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       __syncthreads();
-      pass_u<NT, RQ>(X4, n0, n1, nkq, s.A, s.C, s.M, U, R);
+      pass_u<NT, RQ>(X4, n0, n1, nkq, s.A, s.Ct, s.M, U, R);
       __syncthreads();
       ok = solve_mode<NT>(s, s.M, n1, R, Rp, s.GA, s.GC, s.B, s.GB, ridge_eps, &ridge_used);
     }
@@ -379,6 +399,7 @@ __device__ void run_instance(const BatchArgs& a, int id, unsigned char* smem_raw
       }
       __syncthreads();
       ok = solve_mode<NT>(s, s.M, n2p, R, Rp, s.GA, s.GB, s.C, s.GC, ridge_eps, &ridge_used);
+      transpose_c(s, n2p, Rp, NT);  // the next sweep's passes read the new C through Ct
     }
     if (!ok) {
       if (threadIdx.x == 0) {
