@@ -30,7 +30,7 @@ struct tsr_dense {
   void* owned[2 * tsr::kMaxModes + 2] = {};
   tsr::ModeOperand ops[tsr::kMaxModes];
   double* d_scalars = nullptr;  // [0] ||X||^2, [1] <X, Xhat>, [2] loss, [3] scratch
-  // BF16x3 tensors of 4 or more modes whose trailing-two-modes view
+  // BF16x3 tensors of 3 or more modes whose trailing-two-modes view
   // (prod of the leading modes, I_{N-2}, I_{N-1}) suits the two-sided
   // contraction or the single-layout 3-way MTTKRP: X's bf16 halves in its own
   // layout (owned[2N], owned[2N+1])
@@ -781,11 +781,12 @@ int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, cons
   }
   if (cudaMalloc(&d->d_scalars, 4 * sizeof(double)) != cudaSuccess)
     return cleanup(fail(TSR_E_CUDA, "cudaMalloc of the loss scalars failed"));
-  // BF16x3, 4+ modes: the trailing-two-modes view for the single-layout kernel
+  // BF16x3, 3+ modes: the trailing-two-modes view (with 3 modes the leading
+  // side is mode 0 alone)
   const int64_t vshape[3] = {prod_range(shape, 0, ndim - 2), shape[ndim - 2], shape[ndim - 1]};
   d->d3_three = dense3_supported(3, vshape, 1);
   d->d3_two = twosided_supported(vshape[0], vshape[1] * vshape[2], 1);
-  if (precision == TSR_PREC_BF16X3 && ndim >= 4 && (d->d3_three || d->d3_two) &&
+  if (precision == TSR_PREC_BF16X3 && ndim >= 3 && (d->d3_three || d->d3_two) &&
       vshape[0] <= ((int64_t)1 << 30) &&
       ((uintptr_t)d_tensor & 15) == 0) {
     const int64_t n = numel(ndim, shape);
