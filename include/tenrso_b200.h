@@ -180,9 +180,9 @@ int tsr_gram_inverse_f64(tsr_ctx* ctx, const double* gram, int64_t rank, int ite
  * floats. The stream must belong to the current device (TSR_E_INVALID_ARG
  * otherwise); negative sizes are rejected, and an empty tensor gives a zero
  * output. The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race and must
- * be serialised by the caller. */
+ * (cudaGetSymbolAddress) and sets the kernels' attributes. All calls share
+ * the array, so calls that overlap on the GPU race and must be serialised by
+ * the caller. */
 int tsr_mttkrp_mode0_noalloc_f32(void* stream, const float* d_tensor, int ndim,
                                  const int64_t* shape, const float* const* d_factors,
                                  int64_t rank, float* d_out);
