@@ -72,6 +72,9 @@ __device__ __forceinline__ void gram_rows_accumulate(const float* __restrict__ U
     }
 }
 
+// the state occupies the first 256 bytes of its buffer, the fit history follows
+static_assert(sizeof(AlsState) <= 256, "AlsState must fit its 256-byte slot");
+
 struct AlsBuffers {
   double* grams;    // [N][R][R]   U_m^T U_m
   double* hadam;    // [N][R][R]   Hadamard of the other Grams (G_n)

@@ -111,6 +111,8 @@ struct tsr_ctx {
   tsr::Buffer slots[tsr::SLOT_COUNT];
   void* pinned = nullptr;  // pinned host staging (grow-only)
   size_t pinned_bytes = 0;
+  void* readback = nullptr;  // pinned host buffer for a call's closing read-back (grow-only)
+  size_t readback_bytes = 0;
   unsigned* d_status = nullptr;  // device status word
   int64_t launches = 0;          // kernels launched by this context (counter)
   // clock-cycle budget of each bounded pipeline wait in the tensor-core
@@ -149,6 +151,9 @@ namespace tsr {
 // Grow-only device buffer for a slot; contents are not preserved on growth.
 int slot_get(tsr_ctx* ctx, int slot, size_t bytes, void** out);
 int pinned_get(tsr_ctx* ctx, size_t bytes, void** out);
+// Pinned host buffer for small device-to-host read-backs (grow-only; growing
+// synchronizes the stream first).
+int readback_get(tsr_ctx* ctx, size_t bytes, void** out);
 int check_ctx(tsr_ctx* ctx);
 int read_status(tsr_ctx* ctx, unsigned* out);  // synchronizes the stream
 // Evict L2 by reading a buffer of twice its size (clean lines only).

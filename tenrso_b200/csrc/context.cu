@@ -71,6 +71,22 @@ int pinned_get(tsr_ctx* ctx, size_t bytes, void** out) {
   return TSR_OK;
 }
 
+int readback_get(tsr_ctx* ctx, size_t bytes, void** out) {
+  if (ctx->readback_bytes < bytes) {
+    if (ctx->readback) {
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      TSR_CUDA(cudaFreeHost(ctx->readback));
+      ctx->readback = nullptr;
+      ctx->readback_bytes = 0;
+    }
+    size_t want = (bytes + 4095) & ~size_t(4095);
+    TSR_CUDA(cudaMallocHost(&ctx->readback, want));
+    ctx->readback_bytes = want;
+  }
+  *out = ctx->readback;
+  return TSR_OK;
+}
+
 // Read-only L2 flush: streams a buffer of twice the L2 size through ordinary
 // loads, leaving L2 full of clean lines (a memset flush leaves dirty lines
 // whose write-back the next kernel would pay for). The buffer's contents are
@@ -437,6 +453,7 @@ int tsr_ctx_destroy(tsr_ctx* ctx) {
   for (auto& b : ctx->slots)
     if (b.ptr) cudaFree(b.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->readback) cudaFreeHost(ctx->readback);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->trace_start) cudaFree(ctx->trace_start);
   for (auto& g : ctx->sweep_graphs)

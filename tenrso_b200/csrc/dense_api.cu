@@ -635,9 +635,25 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     }
   }
   if (max_iters > 0) TSR_TRY(launch_fit(ctx, ctx->stream, a.b, ndim, R, tol));
+  // one read-back into pinned memory, one synchronization: the state with the
+  // fit history behind it (SLOT_STATE: state at 0, history at 256) and the
+  // MTTKRP kernels' status word
+  const size_t hist_bytes = sizeof(double) * (size_t)std::max(max_iters, 0);
+  void* rbp;
+  TSR_TRY(readback_get(ctx, 256 + hist_bytes + 16, &rbp));
+  uint8_t* rb = (uint8_t*)rbp;
+  TSR_CUDA(cudaMemcpyAsync(rb, a.b.state, 256 + hist_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaMemcpyAsync(rb + 256 + hist_bytes, ctx->d_status, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  TSR_CUDA(cudaStreamSynchronize(ctx->stream));
   AlsState hs;
-  TSR_CUDA(cudaMemcpyAsync(&hs, a.b.state, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
-  TSR_TRY(check_device_status(ctx));  // synchronizes; a timed-out MTTKRP wait
+  std::memcpy(&hs, rb, sizeof(hs));
+  unsigned mst = 0;
+  std::memcpy(&mst, rb + 256 + hist_bytes, sizeof(mst));
+  if (mst) {
+    TSR_TRY(reset_status(ctx));
+    if (mst & DS_TIMEOUT) return fail(TSR_E_TIMEOUT, "device wait timed out in the MTTKRP kernel");
+  }
   if (hs.status & DS_TIMEOUT)
     return fail(TSR_E_TIMEOUT, "device wait timed out in the CP-ALS sweep");
   if (hs.status & DS_NOT_SPD)
@@ -656,8 +672,7 @@ int cp_als_device(tsr_ctx* ctx, const float* dX, const tsr_sparse* sp, int ndim,
     info->final_fit_change = hs.final_change;
     info->ridge_used = hs.ridge_used;
     if (info->fit_history && hs.iter > 0)
-      TSR_CUDA(cudaMemcpy(info->fit_history, a.b.history, sizeof(double) * hs.iter,
-                          cudaMemcpyDeviceToHost));
+      std::memcpy(info->fit_history, rb + 256, sizeof(double) * std::min(hs.iter, max_iters));
   }
   return TSR_OK;
 }
