@@ -20,8 +20,17 @@ torch.distributed (NCCL between GPUs; gloo, on host copies, between processes
 that share a GPU or run on CPU).
 
 The compute is a backend: DeviceBackend runs the library's MTTKRP and FP64
-solve kernels on this process's GPU. Any object with the same four methods
-(mttkrp, solve, norm_sq, to_host) can stand in for it.
+solve kernels on this process's GPU. Any object with the same methods (put,
+mttkrp, solve, norm_sq, to_host) can stand in for it.
+
+The same partition serves the other sharded paths:
+  cp_als_sparse_sharded   a COO tensor, each rank keeping the nonzeros of its
+                          mode-0 slab (SparseDeviceBackend: the CSF MTTKRP);
+  loss_grad_sharded       the loss and every gradient of ||X - [[U]]||^2 +
+                          reg sum ||U_n||^2: partial MTTKRPs of modes >= 1 and
+                          the slab scalars summed, dL/dU_0 rows all-gathered;
+  batched_cp_als_sharded  independent instances partitioned by work, no
+                          collective.
 """
 from __future__ import annotations
 
@@ -221,3 +230,200 @@ def cp_als_sharded(X_slab, n_rows_total: int, rank: int, max_iters: int, tol: fl
     conv = ConvergenceInfo(fit_history=np.asarray(hist), reason=REASONS[reason],
                            oscillated=osc > 0, oscillation_count=osc, final_fit_change=change)
     return ShardedCpDecomp(factors=factors, fit=fit, iters=iters, convergence=conv)
+
+
+# ---------------------------------------------------------------------------
+# Sparse slabs: the nonzeros of a mode-0 slab, behind the same backend methods
+
+
+class SparseSlab:
+    """The nonzeros of rows [r0, r1) of mode 0, with mode-0 indices made
+    local (i0 - r0); `sp` is the device tensor (None when the slab holds no
+    nonzero). shape / ndim describe the local slab."""
+
+    def __init__(self, indices: np.ndarray, values: np.ndarray, shape: Sequence[int], r0: int,
+                 r1: int, ctx=None):
+        idx = np.asarray(indices, np.int64).reshape(-1, len(shape))
+        vals = np.asarray(values, np.float32)
+        keep = (idx[:, 0] >= r0) & (idx[:, 0] < r1)
+        idx = idx[keep].copy()
+        idx[:, 0] -= r0
+        vals = vals[keep]
+        self.shape = [r1 - r0] + [int(s) for s in shape[1:]]
+        self.ndim = len(shape)
+        self.nnz = int(vals.size)
+        # ||X||^2 of the merged tensor: duplicates summed in fp32 in their
+        # order, as the device tensor merges them (coo.rs:320-347)
+        merged = vals
+        if self.nnz:
+            keys = np.ravel_multi_index(tuple(idx.T), self.shape)
+            order = np.argsort(keys, kind="stable")
+            _, starts = np.unique(keys[order], return_index=True)
+            merged = np.add.reduceat(vals[order], starts).astype(np.float32)
+        self.norm_sq = float(np.sum(merged.astype(np.float64) ** 2))
+        self.sp = None
+        if self.nnz and self.shape[0] > 0:
+            from .sparse import CooTensor, SparseTensor
+            self.sp = SparseTensor(CooTensor(idx, vals, self.shape), ctx=ctx)
+
+    def close(self):
+        if self.sp is not None:
+            self.sp.close()
+            self.sp = None
+
+
+class SparseDeviceBackend(DeviceBackend):
+    """The library's CSF MTTKRP (tsr_mttkrp_csf_dev_f32) on this process's GPU
+    for a SparseSlab; the FP64 solve as DeviceBackend."""
+
+    def mttkrp(self, X: SparseSlab, factors, mode: int):
+        torch = self.torch
+        R = factors[0].shape[1]
+        out = torch.zeros(X.shape[mode], R, dtype=torch.float32, device=factors[-1].device)
+        if X.sp is not None:
+            X.sp.mttkrp_dev([f.data_ptr() for f in factors], R, mode, out.data_ptr())
+        return out
+
+    def norm_sq(self, X: SparseSlab) -> float:
+        return X.norm_sq
+
+
+def cp_als_sparse_sharded(indices, values, shape, rank: int, max_iters: int, tol: float,
+                          init_factors: Sequence[np.ndarray], backend=None, group=None,
+                          dist=None) -> ShardedCpDecomp:
+    """CP-ALS of a sparse tensor (COO: indices nnz x ndim, values) sharded by
+    mode-0 slabs: each rank keeps the nonzeros of its rows slab_rows(shape[0],
+    world, rank) and runs cp_als_sharded with the CSF MTTKRP as its compute.
+    Equals cp_als on the tensor with its zeros (core.rs:59-182)."""
+    if dist is None:
+        import torch.distributed as tdist
+        dist = tdist if tdist.is_available() and tdist.is_initialized() else None
+    world = dist.get_world_size(group) if dist else 1
+    me = dist.get_rank(group) if dist else 0
+    r0, r1 = slab_rows(int(shape[0]), world, me)
+    be = backend if backend is not None else SparseDeviceBackend()
+    slab = SparseSlab(indices, values, shape, r0, r1,
+                      ctx=getattr(be, "ctx", None)) if isinstance(be, SparseDeviceBackend) \
+        else be.slab(indices, values, shape, r0, r1)
+    try:
+        return cp_als_sharded(slab, int(shape[0]), rank, max_iters, tol, init_factors, backend=be,
+                              group=group, dist=dist)
+    finally:
+        if isinstance(slab, SparseSlab):
+            slab.close()
+
+
+# ---------------------------------------------------------------------------
+# The loss / gradient of ||X - [[U]]||^2 + reg sum ||U_n||^2 by mode-0 slabs
+
+
+def _all_gather_rows(u: np.ndarray, n_rows_total: int, dist, group) -> np.ndarray:
+    """The full row-stacked matrix from every rank's slab rows."""
+    import torch
+    if dist is None:
+        return u
+    world = dist.get_world_size(group)
+    if world == 1:
+        return u
+    counts = [slab_rows(n_rows_total, world, p) for p in range(world)]
+    width = max(b - a for a, b in counts)
+    buf = np.zeros((width, u.shape[1]), u.dtype)
+    buf[:u.shape[0]] = u
+    t = torch.from_numpy(buf)
+    if dist.get_backend(group) == "nccl":
+        t = t.cuda()
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t, group=group)
+    return np.concatenate([p.cpu().numpy()[:b - a] for p, (a, b) in zip(parts, counts)])
+
+
+def loss_grad_sharded(X_slab, n_rows_total: int, factors: Sequence[np.ndarray], reg: float,
+                      backend=None, group=None, dist=None):
+    """(loss, [dL/dU_n]) of ||X - [[U]]||^2 + reg sum_n ||U_n||^2 with X held
+    by mode-0 slabs (this rank: rows slab_rows(n_rows_total, world, rank)) and
+    every factor replicated. Gram form, as tsr_cp_loss_grad_dev_f32:
+      dL/dU_n = 2 (U_n H_n - M_n + reg U_n),  H_n = *_{m != n} U_m^T U_m,
+      loss = ||X||^2 - 2 <M_0, U_0> + sum prod_n Gram_n + reg sum_n tr(Gram_n).
+    Exchanges: the partial MTTKRPs M_n of modes n >= 1, U_0's partial Gram and
+    the slab scalars are summed over ranks (FP64), dL/dU_0's rows all-gathered.
+    Every rank returns the full loss and gradients (FP64 host arrays)."""
+    if dist is None:
+        import torch.distributed as tdist
+        dist = tdist if tdist.is_available() and tdist.is_initialized() else None
+    world = dist.get_world_size(group) if dist else 1
+    me = dist.get_rank(group) if dist else 0
+    be = backend if backend is not None else DeviceBackend()
+    r0, r1 = slab_rows(n_rows_total, world, me)
+    X = X_slab if not isinstance(X_slab, np.ndarray) else be.put(X_slab)
+    if X.shape[0] != r1 - r0:
+        raise ValueError(f"slab has {X.shape[0]} rows, rank {me} of {world} owns {r1 - r0}")
+    N = len(factors)
+    R = int(np.asarray(factors[0]).shape[1])
+    if R == 0:
+        raise TenrsoError(5, f"Invalid rank: {R}")
+    U = [be.put(np.asarray(factors[0])[r0:r1])] + [be.put(np.asarray(f)) for f in factors[1:]]
+    Uh = [np.asarray(be.to_host(u), np.float64) for u in U]
+    grams = [u.T @ u for u in Uh]
+    grams[0] = _allreduce_sum(grams[0], dist, group)
+    M = []
+    for n in range(N):
+        m = np.asarray(be.to_host(be.mttkrp(X, U, n)), np.float64)
+        M.append(m if n == 0 else _allreduce_sum(m, dist, group))
+    scal = np.array([be.norm_sq(X), float(np.sum(M[0] * Uh[0]))])
+    scal = _allreduce_sum(scal, dist, group)
+    grads = []
+    for n in range(N):
+        H = np.ones((R, R))
+        for m in range(N):
+            if m != n:
+                H = H * grams[m]
+        grads.append(2.0 * (Uh[n] @ H - M[n] + reg * Uh[n]))
+    H = np.ones((R, R))
+    for g in grams:
+        H = H * g
+    loss = float(scal[0] - 2.0 * scal[1] + H.sum() + reg * sum(np.trace(g) for g in grams))
+    grads[0] = _all_gather_rows(grads[0], n_rows_total, dist, group)
+    return loss, grads
+
+
+# ---------------------------------------------------------------------------
+# Batched CP-ALS: independent instances partitioned over ranks
+
+
+def partition_instances(work: Sequence[float], world: int) -> List[List[int]]:
+    """Instance ids per rank: largest work first, each to the rank with the
+    least work so far (ties to the lower rank); ids ascending within a rank."""
+    order = sorted(range(len(work)), key=lambda i: (-float(work[i]), i))
+    loads = [0.0] * world
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        p = min(range(world), key=lambda q: (loads[q], q))
+        parts[p].append(i)
+        loads[p] += float(work[i])
+    return [sorted(p) for p in parts]
+
+
+def batched_cp_als_sharded(tensors: Sequence[np.ndarray], ranks: Sequence[int], max_iters: int,
+                           tol: float, inits: Sequence[Sequence[np.ndarray]], group=None,
+                           dist=None, ctx=None):
+    """This rank's share of a batch of independent CP-ALS instances (no
+    collective): partition_instances by n0 n1 n2 R work, then one
+    BatchedCpAls run over the rank's instances. Returns (ids, results) with
+    results[k] the CpDecomp of instance ids[k]."""
+    if dist is None:
+        import torch.distributed as tdist
+        dist = tdist if tdist.is_available() and tdist.is_initialized() else None
+    world = dist.get_world_size(group) if dist else 1
+    me = dist.get_rank(group) if dist else 0
+    work = [float(np.prod(np.asarray(t).shape)) * r for t, r in zip(tensors, ranks)]
+    ids = partition_instances(work, world)[me]
+    if not ids:
+        return [], []
+    from .batched import BatchedCpAls
+    b = BatchedCpAls([np.asarray(tensors[i], np.float32) for i in ids], [ranks[i] for i in ids],
+                     ctx=ctx)
+    try:
+        out = b.cp_als(max_iters, tol, init=[inits[i] for i in ids])
+    finally:
+        b.close()
+    return ids, out
