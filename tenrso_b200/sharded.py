@@ -279,9 +279,15 @@ class SparseDeviceBackend(DeviceBackend):
     def mttkrp(self, X: SparseSlab, factors, mode: int):
         torch = self.torch
         R = factors[0].shape[1]
-        out = torch.zeros(X.shape[mode], R, dtype=torch.float32, device=factors[-1].device)
-        if X.sp is not None:
-            X.sp.mttkrp_dev([f.data_ptr() for f in factors], R, mode, out.data_ptr())
+        if X.sp is None:
+            return torch.zeros(X.shape[mode], R, dtype=torch.float32, device=factors[-1].device)
+        # the CSF MTTKRP writes every output row on the library context's own
+        # stream and returns without synchronizing: order it against torch's
+        # stream on both sides
+        out = torch.empty(X.shape[mode], R, dtype=torch.float32, device=factors[-1].device)
+        torch.cuda.synchronize()
+        X.sp.mttkrp_dev([f.data_ptr() for f in factors], R, mode, out.data_ptr())
+        torch.cuda.synchronize()
         return out
 
     def norm_sq(self, X: SparseSlab) -> float:

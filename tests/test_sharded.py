@@ -40,9 +40,9 @@ if kind == "sparse_cp_als":
     sys.path.insert(0, os.path.join(os.environ["SHARD_ROOT"], "tests"))
     from test_sharded import merged_zipf_coo
     X = merged_zipf_coo(shape, cfg["nnz"], cfg["seed"])
-else:
+elif kind != "batched":  # the batched instances are drawn below
     X, _ = synth.dense_lowrank(shape, R, seed=cfg["seed"], dist="normal", noise=0.01)
-init = synth.init_factors(shape, R, cfg["seed"])
+init = synth.init_factors(shape, R, cfg["seed"]) if kind != "batched" else None
 r0, r1 = slab_rows(shape[0], world, me)
 
 if kind == "loss_grad":
