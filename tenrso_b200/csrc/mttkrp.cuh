@@ -59,9 +59,7 @@ int launch_split_bf16(tsr_ctx* ctx, cudaStream_t s, const float* X, int64_t n, _
 // L_img > L: the image covers L_img rows, those from L on zero.
 int launch_bimage(tsr_ctx* ctx, cudaStream_t s, const float* U, int64_t L, int R, int n_pad,
                   uint8_t* img, int64_t L_img = 0);
-// SplitPlan: splits, k_per_split = k-steps (runs x 64-wide k-blocks, run-major)
-// per split, a range that may start and end inside a run; run_length =
-// contracted length.
+// SplitPlan: splits, k_per_split = runs per split, run_length = contracted length.
 SplitPlan plan_mttkrp3(const tsr_ctx* ctx, const Dense3& d, int mode);
 // Partials [splits][rows][R] of mode `mode`; the weights come from ft.
 int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, const FactorTable& ft,

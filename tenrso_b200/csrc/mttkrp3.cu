@@ -64,7 +64,7 @@ struct M3Params {
   int64_t rows;         // M: I, J or K
   int64_t runs;         // runs in total: J (mode 0) or I
   int L;                // contracted length: K (modes 0, 1) or J (mode 2)
-  int steps_per_split;   // k-steps (runs x k-blocks, run-major) per CTA
+  int runs_per_split;
   int R;
   int n_pad;            // 32 or 64
   int stages;
@@ -136,17 +136,10 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t m0 = (int64_t)blockIdx.y * M3_BM;
-  // this CTA's global k-steps [g0, g1) (step g = run * spr + k-block): it
-  // may start and end inside a run; a partial run's sum is scaled by the
-  // run's weight row like a whole one
-  const int64_t total_steps = p.runs * spr;
-  const int64_t g0 = (int64_t)blockIdx.x * p.steps_per_split;
-  const int64_t g1 = g0 + p.steps_per_split < total_steps ? g0 + p.steps_per_split : total_steps;
-  const int nsteps = g1 > g0 ? (int)(g1 - g0) : 0;
-  const int64_t run0 = g0 / spr;
-  const int nruns = nsteps > 0 ? (int)((g1 - 1) / spr - run0 + 1) : 0;
-  const int k_first = (int)(g0 - run0 * spr);            // first k-block of the first run
-  const int k_last = nsteps > 0 ? (int)((g1 - 1) % spr) + 1 : 0;  // end of the last run's
+  const int64_t run0 = (int64_t)blockIdx.x * p.runs_per_split;
+  const int64_t left = p.runs - run0;
+  const int nruns = left <= 0 ? 0 : (int)(left < p.runs_per_split ? left : p.runs_per_split);
+  const int nsteps = nruns * spr;
   const int acc_cols = 2 * p.n_pad;  // one accumulator: hh | cr
   const int tmem_cols = 2 * acc_cols;
   trace_begin(p.tr);
@@ -194,9 +187,8 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
         }
         uint8_t* st = a_base + (size_t)s * 2 * M3_A_TILE;
         mbar_arrive_expect_tx(&tma_full[s], 2u * M3_A_TILE);
-        const int64_t g = g0 + it;
-        const int32_t kb = (int32_t)((g % spr) * M3_BK);
-        const int32_t run = (int32_t)(g / spr);
+        const int32_t kb = (int32_t)((it % spr) * M3_BK);
+        const int32_t run = (int32_t)(run0 + it / spr);
         const int32_t m = (int32_t)m0;
         if (p.mode == 0) {  // box (64 k, 1 j, 128 i)
           tma_load_3d_hint(st, &map_hi, kb, run, m, &tma_full[s], pol);
@@ -226,7 +218,6 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
       const uint32_t amaj = p.mode == 2 ? (1u << 15) : 0u;  // transpose A: MN-major
       const uint32_t idesc = idesc_bf16_f32(M3_BM, 2 * p.n_pad) | amaj;
       bool ok = nruns == 0 || m3_wait(b_full, 0, abort_flag, p.wait_budget);
-      int it = 0;  // ring position: this CTA's step count so far
       for (int r = 0; ok && r < nruns; ++r) {
         const int b = r & 1;
         // buffer b was last used by run r - 2: wait until the epilogue read it
@@ -237,8 +228,8 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
         }
         tc_fence_after();
         const uint32_t acc = tmem + (uint32_t)(b * acc_cols);
-        const int sp0 = r == 0 ? k_first : 0, sp1 = r == nruns - 1 ? k_last : spr;
-        for (int sp = sp0; sp < sp1; ++sp, ++it) {
+        for (int sp = 0; sp < spr; ++sp) {
+          const int it = r * spr + sp;
           const int s = it % S;
           const uint32_t ph = (uint32_t)(it / S) & 1u;
           if (!m3_wait(&tma_full[s], ph, abort_flag, p.wait_budget)) {
@@ -260,7 +251,7 @@ mttkrp3_kernel(const __grid_constant__ CUtensorMap map_hi,
               dal = desc_sw128_kmajor(a_lo + kk * 32u);
             }
             const uint64_t db = desc_sw128_kmajor(bt + kk * 32u);
-            const uint32_t first = (sp == sp0 && kk == 0) ? 0u : 1u;
+            const uint32_t first = (sp == 0 && kk == 0) ? 0u : 1u;
             // both products accumulate into the whole accumulator: an MMA into
             // a column range that only overlaps the previous one serialises the
             // tensor pipe, one into the same range pipelines
@@ -956,17 +947,13 @@ SplitPlan plan_mttkrp3(const tsr_ctx* ctx, const Dense3& d, int mode) {
   SplitPlan p;
   const int64_t rows = mode == 0 ? d.I : (mode == 1 ? d.J : d.K);
   const int64_t runs = mode == 0 ? d.J : d.I;
-  const int L = mode == 2 ? (int)d.J : (int)d.K;
-  const int64_t spr = ceil_div(L, M3_BK);
-  const int64_t total = runs * spr;
   const int64_t mt = ceil_div(rows, M3_BM);
   const int64_t want = std::max<int64_t>(1, (ctx->sm_count - ctx->reserve_sms) / mt);
-  int64_t per = ceil_div(total, std::min<int64_t>(want, total));
-  // a range of `per` steps touches at most per / spr + 2 runs (weight rows)
-  per = std::min<int64_t>(per, (M3_MAX_RUNS - 2) * spr);
-  p.splits = (int)ceil_div(total, per);
-  p.k_per_split = per;  // k-steps per split
-  p.run_length = L;
+  int64_t per = ceil_div(runs, std::min<int64_t>(want, runs));
+  per = std::min<int64_t>(per, M3_MAX_RUNS);
+  p.splits = (int)ceil_div(runs, per);
+  p.k_per_split = per;  // runs per split
+  p.run_length = mode == 2 ? (int)d.J : (int)d.K;
   return p;
 }
 
@@ -983,7 +970,7 @@ int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, cons
   q.rows = dense3_rows(d, mode);
   q.runs = mode == 0 ? d.J : d.I;
   q.L = mode == 2 ? (int)d.J : (int)d.K;
-  q.steps_per_split = (int)plan.k_per_split;
+  q.runs_per_split = (int)plan.k_per_split;
   q.R = d.R;
   q.n_pad = d.n_pad;
   // the contracted factor's image: U2 for modes 0 and 1, U1 for mode 2
@@ -995,8 +982,7 @@ int launch_mttkrp3(tsr_ctx* ctx, cudaStream_t s, const Dense3& d, int mode, cons
   q.wait_budget = ctx->wait_budget;
   q.a_resident = a_resident ? 1 : 0;
   q.tr = trace_slot(ctx, TRACE_MTTKRP, mode);
-  if (q.steps_per_split < 1 ||
-      q.steps_per_split > (M3_MAX_RUNS - 2) * (int)ceil_div(q.L, M3_BK))
+  if (q.runs_per_split < 1 || q.runs_per_split > M3_MAX_RUNS)
     return fail(TSR_E_INVALID_ARG, "MTTKRP split plan out of range");
   int stages = 4;
   while (stages > 2 && m3_smem(d, mode, stages) > (size_t)kM3MaxSmem) --stages;
