@@ -415,6 +415,9 @@ t_contract_grad_kernel(const __grid_constant__ TContract c, const __grid_constan
   __shared__ double part[256];
   __shared__ double H[32 * 32];
   __shared__ double Mrow[32];
+  // programmatic launch: T, P and, through the earlier kernels' own waits,
+  // the Grams are complete once the predecessor is
+  grid_dep_wait();
   const int b = blockIdx.x;
   const int R = c.R;
   if (b >= c.row0[c.nmodes]) {
@@ -850,6 +853,7 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
   void* gp;
   TSR_TRY(slot_get(ctx, SLOT_GRAMS, sizeof(double) * N * RR, &gp));
   double* grams = (double*)gp;
+  TSR_CUDA(cudaMemsetAsync(X->d_scalars + 1, 0, 2 * sizeof(double), ctx->stream));
   {
     // every mode's Gram in one launch
     TSR_CUDA(cudaMemsetAsync(grams, 0, sizeof(double) * N * RR, ctx->stream));
@@ -879,7 +883,6 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     ctx->launches++;
     TSR_CUDA(cudaGetLastError());
   }
-  TSR_CUDA(cudaMemsetAsync(X->d_scalars + 1, 0, 2 * sizeof(double), ctx->stream));
   auto grad_of = [&](int n, const float* partials, int splits) -> int {
     const int64_t rows = X->shape[n];
     const int rpc =
@@ -935,9 +938,16 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
       im.chunks = (int)((w == 0 ? vb : wb) / 16);
       im.img = (uint8_t*)ip + (w == 0 ? 0 : vb);
     }
-    TSR_TRY(launch_kr_images(ctx, ctx->stream, ki));
-    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * (A + C) * R, &tp));
-    TSR_CUDA(cudaMemsetAsync(tp, 0, sizeof(float) * (A + C) * R, ctx->stream));
+    // T and P (accumulated into by the two-sided kernel) are zeroed by the
+    // same launch, whole float4s (the slot is padded to them)
+    const int64_t tp_n4 = ceil_div((A + C) * R, 4);
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * 4 * tp_n4, &tp));
+    ki.zero = (float*)tp;
+    ki.zero_n4 = tp_n4;
+    // programmatic launches from here to the end of the evaluation: each
+    // kernel's launch and prologue overlap its predecessor, whose writes it
+    // awaits before reading them
+    TSR_TRY(launch_kr_images(ctx, ctx->stream, ki, true));
     TwoSided ts;
     ts.hi = X->d3.hi;
     ts.lo = X->d3.lo;
@@ -969,7 +979,8 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     g.reg = reg;
     g.scal = X->d_scalars;
     for (int m = 0; m < N; ++m) g.G[m] = d_grads[m];
-    t_contract_grad_kernel<<<(unsigned)total_rows + 1, 256, 0, ctx->stream>>>(c, g);
+    TSR_CUDA(launch_pdl(t_contract_grad_kernel, dim3((unsigned)total_rows + 1), dim3(256), 0,
+                        ctx->stream, c, g));
     ctx->launches++;
     TSR_CUDA(cudaGetLastError());
     if (loss) {

@@ -97,10 +97,16 @@ struct KRImages {
   KRImage im[2];
   int n;  // images in use (1 or 2)
   int R, n_pad;
+  float* zero;      // also zero-filled by the launch: zero_n4 float4s (16-byte aligned)
+  int64_t zero_n4;
 };
-int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a);
+// pdl: programmatic dependent launch (the kernel waits for its predecessor
+// before writing, then lets its dependent start).
+int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a, bool pdl = false);
 bool twosided_supported(int64_t A, int64_t C, int R);
 int64_t twosided_pad(int64_t L);
+// Launched with programmatic dependent launch: the prologue overlaps the
+// predecessor, whose writes are awaited before any operand is read.
 int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a);
 
 // Materialised two-factor Khatri-Rao product (the public khatri_rao API).

@@ -474,12 +474,21 @@ __global__ void bimage_kernel(const float* __restrict__ U, int L, int R, int n_p
 // images per launch: row k of a product is the row-major multi-index over its
 // factors' rows, each entry the fp32 product of the factors' entries.
 __global__ void kr_images_kernel(const __grid_constant__ KRImages a) {
+  // programmatic launch: the predecessor's writes first (no-ops for a plain
+  // launch); the next kernel may then start its own prologue
+  grid_dep_wait();
+  if (threadIdx.x == 0) grid_dep_trigger();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   int w = 0;
   if (e >= a.im[0].chunks) {
     e -= a.im[0].chunks;
     w = 1;
-    if (a.n < 2 || e >= a.im[1].chunks) return;
+    if (a.n < 2 || e >= a.im[1].chunks) {
+      // the threads past both images zero `zero` (float4s)
+      const int64_t z = (int64_t)e - (a.n < 2 ? 0 : a.im[1].chunks);
+      if (z >= 0 && z < a.zero_n4) reinterpret_cast<float4*>(a.zero)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
+    }
   }
   const KRImage& im = a.im[w];
   const int pos = e & 7;
@@ -708,6 +717,7 @@ twosided_kernel(const __grid_constant__ CUtensorMap map_hi,
   const int cleft = p.ncb - cb0;
   const int nc = cleft <= 0 ? 0 : (cleft < p.cb_per_split ? cleft : p.cb_per_split);
   const int nsteps = nta > 0 ? nc * nta : 0;
+  if (threadIdx.x == 0) grid_dep_trigger();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -733,6 +743,9 @@ twosided_kernel(const __grid_constant__ CUtensorMap map_hi,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // programmatic launch: the prologue above overlapped the predecessor; its
+  // writes (the B images, the zeroed T and P) are complete from here on
+  grid_dep_wait();
 
   if (warp == 0) {
     if (lane == 0) {
@@ -1005,9 +1018,11 @@ bool twosided_supported(int64_t A, int64_t C, int R) {
 
 int64_t twosided_pad(int64_t L) { return ceil_div(L, 128) * 128; }
 
-int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a) {
+int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a, bool pdl) {
   if (a.n < 1 || a.n > 2) return fail(TSR_E_INVALID_ARG, "one or two images per launch");
-  int64_t total = 0;
+  if (a.zero_n4 < 0 || (a.zero_n4 > 0 && ((uintptr_t)a.zero & 15)))
+    return fail(TSR_E_INVALID_ARG, "zero-fill buffer misaligned");
+  int64_t total = a.zero_n4;
   for (int w = 0; w < a.n; ++w) {
     if (a.im[w].nf < 1 || a.im[w].nf > kMaxModes)
       return fail(TSR_E_INVALID_ARG, "Khatri-Rao image of %d factors", a.im[w].nf);
@@ -1017,7 +1032,10 @@ int launch_kr_images(tsr_ctx* ctx, cudaStream_t s, const KRImages& a) {
     total += a.im[w].chunks;
   }
   if (total <= 0) return TSR_OK;
-  kr_images_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, s>>>(a);
+  if (pdl)
+    TSR_CUDA(launch_pdl(kr_images_kernel, dim3((unsigned)ceil_div(total, 256)), dim3(256), 0, s, a));
+  else
+    kr_images_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, s>>>(a);
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
@@ -1045,7 +1063,8 @@ int launch_twosided(tsr_ctx* ctx, cudaStream_t s, const TwoSided& a) {
   q.P = a.P;
   q.status = ctx->d_status;
   q.wait_budget = ctx->wait_budget;
-  twosided_kernel<<<dim3((unsigned)splits, (unsigned)nag), TS_THREADS, TS_SMEM, s>>>(mh, ml, q);
+  TSR_CUDA(launch_pdl(twosided_kernel, dim3((unsigned)splits, (unsigned)nag), dim3(TS_THREADS),
+                      TS_SMEM, s, mh, ml, q));
   ctx->launches++;
   TSR_CUDA(cudaGetLastError());
   return TSR_OK;
