@@ -774,7 +774,7 @@ int tsr_mttkrp_all_modes_f32(tsr_ctx* ctx, const float* tensor, int ndim, const 
   TSR_TRY(check_precision(precision));
   TSR_TRY(check_ctx(ctx));
   const int R = (int)rank;
-  float* dX;
+  float* dX = nullptr;
   TSR_TRY(upload_tensor(ctx, tensor, ndim, shape, nullptr, &dX));
   FactorTable ft{};
   TSR_TRY(upload_factors(ctx, ndim, shape, factors, R, &ft));
@@ -1043,7 +1043,7 @@ int tsr_cp_als_constrained_f32(tsr_ctx* ctx, const float* tensor, int ndim, cons
     }
     init = init_buf.data();
   }
-  float* dX;
+  float* dX = nullptr;
   TSR_TRY(upload_tensor(ctx, tensor, ndim, shape, nullptr, &dX));
   void* df;
   TSR_TRY(slot_get(ctx, SLOT_OUT, sizeof(float) * ftotal, &df));
