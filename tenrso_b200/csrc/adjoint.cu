@@ -27,7 +27,7 @@ struct tsr_dense {
   int precision = 0;
   int device = 0;
   const float* dX = nullptr;
-  void* owned[2 * tsr::kMaxModes + 2] = {};
+  void* owned[2 * tsr::kMaxModes + 4] = {};
   tsr::ModeOperand ops[tsr::kMaxModes];
   double* d_scalars = nullptr;  // [0] ||X||^2, [1] <X, Xhat>, [2] loss, [3] scratch
   // BF16x3 tensors of 3 or more modes whose trailing-two-modes view
@@ -38,6 +38,12 @@ struct tsr_dense {
   bool d3_three = false;  // the view suits the single-layout 3-way MTTKRP
   bool d3_two = false;    // the view suits the two-sided contraction
   tsr::Dense3 d3{};
+  // FP32 tensors of 3 or more modes: the same view as a 2-way tensor
+  // (A, C = I_{N-2} I_{N-1}); its mode-0 operand is X (or a padded copy), its
+  // mode-1 operand the transposed copy (owned[2N + 2], owned[2N + 3])
+  bool v2_on = false;
+  int64_t v2_shape[2] = {0, 0};
+  tsr::ModeOperand vops[2];
 };
 
 namespace tsr {
@@ -810,6 +816,25 @@ int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, cons
     d->d3.hi = (const __nv_bfloat16*)hp;
     d->d3.lo = (const __nv_bfloat16*)lp;
   }
+  if (precision == TSR_PREC_FP32 && ndim >= 3 && vshape[0] <= ((int64_t)1 << 30) &&
+      vshape[1] * vshape[2] < INT32_MAX) {
+    const int64_t v2[2] = {vshape[0], vshape[1] * vshape[2]};
+    for (int m = 0; m < 2; ++m) {
+      size_t ab, bb;
+      mode_operand_bytes(make_unfolding(2, v2, m), precision, &ab, &bb);
+      void* buf = nullptr;
+      if (ab) {
+        if (cudaMalloc(&buf, ab) != cudaSuccess)
+          return cleanup(fail(TSR_E_CUDA, "cudaMalloc of %zu bytes failed", ab));
+        d->owned[2 * kMaxModes + 2 + m] = buf;
+      }
+      int rc = prepare_mode_into(ctx, d_tensor, 2, v2, m, precision, buf, nullptr, &d->vops[m]);
+      if (rc != TSR_OK) return cleanup(rc);
+    }
+    d->v2_on = true;
+    d->v2_shape[0] = v2[0];
+    d->v2_shape[1] = v2[1];
+  }
   cudaError_t e = cudaMemsetAsync(d->d_scalars, 0, 4 * sizeof(double), ctx->stream);
   if (e != cudaSuccess) return cleanup(fail(TSR_E_CUDA, "%s", cudaGetErrorString(e)));
   int rc = launch_norm_sq(ctx, ctx->stream, d_tensor, numel(ndim, shape), d->d_scalars);
@@ -911,6 +936,43 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     }
     return TSR_OK;
   };
+  // From T (A x R: the leading modes, the trailing two contracted) and P
+  // (C x R: the trailing two, the leading contracted): every mode's MTTKRP
+  // and gradient rows and the Gram part of the loss in one programmatic
+  // launch (R <= 32), then the loss when requested.
+  auto contract_grad = [&](const float* T, const float* P) -> int {
+    int total_rows = 0;
+    for (int p = 0; p < N; ++p) total_rows += (int)X->shape[p];
+    TContract c{};
+    set_side(c, 0, T, X->shape, 0, N - 2, d_factors);
+    set_side(c, 1, P, X->shape, N - 2, N, d_factors);
+    c.R = R;
+    c.nmodes = N;
+    c.row0[0] = 0;
+    for (int p = 0; p < N; ++p) {
+      c.side_of[p] = p < N - 2 ? 0 : 1;
+      c.pos[p] = p < N - 2 ? p : p - (N - 2);
+      c.row0[p + 1] = c.row0[p] + (int)X->shape[p];
+    }
+    GradArgs g{};
+    g.grams = grams;
+    g.ndim = N;
+    g.reg = reg;
+    g.scal = X->d_scalars;
+    for (int m = 0; m < N; ++m) g.G[m] = d_grads[m];
+    TSR_CUDA(launch_pdl(t_contract_grad_kernel, dim3((unsigned)total_rows + 1), dim3(256), 0,
+                        ctx->stream, c, g));
+    ctx->launches++;
+    TSR_CUDA(cudaGetLastError());
+    if (loss) {
+      TSR_TRY(check_device_status(ctx));
+      double sc[4];
+      TSR_CUDA(cudaMemcpyAsync(sc, X->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
+      *loss = sc[0] - 2.0 * sc[1] + sc[3];
+    }
+    return TSR_OK;
+  };
   if (X->d3_on && X->d3_two && twosided_supported(X->d3.I, X->d3.J * X->d3.K, R)) {
     // one read of X's bf16 halves: T = X_(lead) KR(trailing two) and
     // P = X_(lead)^T KR(leading) from the two-sided contraction, then every
@@ -959,38 +1021,44 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     ts.T = (float*)tp;
     ts.P = (float*)tp + A * R;
     TSR_TRY(launch_twosided(ctx, ctx->stream, ts));
-    int total_rows = 0;
-    for (int p = 0; p < N; ++p) total_rows += (int)X->shape[p];
-    TContract c{};
-    set_side(c, 0, ts.T, X->shape, 0, N - 2, d_factors);
-    set_side(c, 1, ts.P, X->shape, N - 2, N, d_factors);
-    c.R = R;
-    c.nmodes = N;
-    c.row0[0] = 0;
-    for (int p = 0; p < N; ++p) {
-      c.side_of[p] = p < N - 2 ? 0 : 1;
-      c.pos[p] = p < N - 2 ? p : p - (N - 2);
-      c.row0[p + 1] = c.row0[p] + (int)X->shape[p];
+    return contract_grad(ts.T, ts.P);
+  }
+  if (X->v2_on && R <= 32) {
+    // FP32: X as the 2-way tensor (A, C). T is that view's mode-0 MTTKRP with
+    // W = KR(U_{N-2}, U_{N-1}), P its mode-1 MTTKRP with V = KR(U_0 ..
+    // U_{N-3}): two passes over X (the second over its transposed copy)
+    // instead of one per mode, and half the FLOPs of N MTTKRPs
+    const int64_t A = X->v2_shape[0], C = X->v2_shape[1];
+    void *vp, *vq, *wp, *tp;
+    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * A * R, &vp));
+    TSR_TRY(slot_get(ctx, SLOT_MISC3, sizeof(float) * A * R, &vq));
+    TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(float) * C * R, &wp));
+    TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * (A + C) * R, &tp));
+    const float* V = d_factors[0];
+    int64_t vrows = X->shape[0];
+    float* bufs[2] = {(float*)vp, (float*)vq};
+    for (int p = 1; p < N - 2; ++p) {
+      float* dst = bufs[p & 1];
+      TSR_TRY(launch_khatri_rao(ctx, V, vrows, d_factors[p], X->shape[p], R, dst));
+      V = dst;
+      vrows *= X->shape[p];
     }
-    // every mode's MTTKRP and gradient rows, and the Gram part of the loss
-    GradArgs g{};
-    g.grams = grams;
-    g.ndim = N;
-    g.reg = reg;
-    g.scal = X->d_scalars;
-    for (int m = 0; m < N; ++m) g.G[m] = d_grads[m];
-    TSR_CUDA(launch_pdl(t_contract_grad_kernel, dim3((unsigned)total_rows + 1), dim3(256), 0,
-                        ctx->stream, c, g));
-    ctx->launches++;
-    TSR_CUDA(cudaGetLastError());
-    if (loss) {
-      TSR_TRY(check_device_status(ctx));
-      double sc[4];
-      TSR_CUDA(cudaMemcpyAsync(sc, X->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
-      TSR_CUDA(cudaStreamSynchronize(ctx->stream));
-      *loss = sc[0] - 2.0 * sc[1] + sc[3];
+    TSR_TRY(launch_khatri_rao(ctx, d_factors[N - 2], X->shape[N - 2], d_factors[N - 1],
+                              X->shape[N - 1], R, (float*)wp));
+    FactorTable vt{};
+    vt.ptr[0] = V;
+    vt.rows[0] = A;
+    vt.ptr[1] = (const float*)wp;
+    vt.rows[1] = C;
+    float* T = (float*)tp;
+    float* P = T + A * R;
+    for (int v = 0; v < 2; ++v) {
+      float* partials;
+      int splits;
+      TSR_TRY(run_mttkrp_partials(ctx, X->vops[v], vt, R, TSR_PREC_FP32, &partials, &splits));
+      TSR_TRY(launch_mttkrp_reduce(ctx, partials, splits, (v == 0 ? A : C) * R, v == 0 ? T : P));
     }
-    return TSR_OK;
+    return contract_grad(T, P);
   }
   if (X->d3_on && X->d3_three && R <= 64) {
     // three single-layout passes over X's bf16 halves instead of one MTTKRP

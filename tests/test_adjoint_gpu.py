@@ -97,21 +97,23 @@ def test_loss_grad_vs_cpu_vjp(c5_reference, precision):
         assert rel_err(grads[n], grads_ref[n]) <= 1e-5, (n, rel_err(grads[n], grads_ref[n]))
 
 
-# BF16x3 routes of the loss/gradient on 3+ mode tensors (trailing-two-modes
-# view A x J x K, C = J K): the two-sided contraction (R <= 32, C % 8 == 0)
+# Routes of the loss/gradient on 3+ mode tensors (trailing-two-modes view
+# A x J x K, C = J K). BF16x3: the two-sided contraction (R <= 32, C % 8 == 0)
 # with ragged A and C blocks (128), R % 4 != 0, three and five modes and K % 8
 # != 0; the three-pass single-layout view (32 < R <= 64); the per-mode path.
+# FP32: the 2-way view's two MTTKRPs (R <= 32), else one MTTKRP per mode.
 @pytest.mark.parametrize("shape,R", [((10, 9, 8, 16), 7), ((5, 6, 24, 40), 12),
                                      ((3, 4, 5, 6, 16), 8), ((7, 6, 10, 12), 5),
                                      ((6, 5, 8, 16), 40), ((9, 7, 5, 3), 6),
                                      ((200, 24, 56), 16), ((33, 17, 8), 5),
                                      ((40, 24, 56), 48)])
-def test_loss_grad_routes_bf16x3(orc, shape, R):
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_loss_grad_routes(orc, shape, R, precision):
     rng = np.random.default_rng(sum(shape) + R)
     X = rng.standard_normal(shape).astype(np.float32)
     fs = [rng.standard_normal((n, R)).astype(np.float32) for n in shape]
     loss_ref, grads_ref = orc.cp_loss_grad_vjp(X, fs, C5_REG)
-    loss, grads = tb.cp_loss_grad(X, fs, C5_REG, "bf16x3")
+    loss, grads = tb.cp_loss_grad(X, fs, C5_REG, precision)
     assert abs(loss - loss_ref) <= 1e-6 * abs(loss_ref), (loss, loss_ref)
     for n in range(len(shape)):
         assert rel_err(grads[n], grads_ref[n]) <= 1e-5, (n, rel_err(grads[n], grads_ref[n]))
