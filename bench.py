@@ -476,8 +476,8 @@ def run_adjoint(tb, torch, ctx, stream, args, world, dist, rank):
     fptr = [f.data_ptr() for f in dF]
     gptr = [g.data_ptr() for g in dGr]
     steps = max(5, args.steps)
-    # algorithmic bytes: fp32, the 2-way view's two MTTKRP passes (X and its
-    # transposed copy, 2 x 4 B per element); bf16x3, one two-sided read of X's
+    # algorithmic bytes: fp32, two MTTKRP passes (X and its transposed copy,
+    # 2 x 4 B per element); bf16x3, one two-sided read of X's
     # bf16 halves (4 B per element)
     out = {"workload": "CP loss+gradient 128x96x64x48, rank 32, reg 1e-3",
            "bytes_alg_per_eval": {"fp32": 2 * 4 * X.size, "bf16x3": 4 * X.size}}

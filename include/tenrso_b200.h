@@ -462,9 +462,9 @@ int tsr_dense_destroy(tsr_dense* X);
  * counterpart; the gradient equals grad.rs's rule applied to G = 2(Xhat - X)
  * plus 2 reg U_n), evaluated through Gram identities without forming Xhat:
  * one MTTKRP of X per mode plus FP64 R x R work (three or more modes, rank
- * <= 32: BF16x3 one two-sided contraction reading X once, FP32 two MTTKRPs
- * of X seen as a 2-way tensor; BF16x3 rank <= 64: three single-layout
- * passes). d_grads[n]: shape[n] x rank.
+ * <= 32: BF16x3 one two-sided contraction reading X once, FP32 two
+ * MTTKRPs, of X and of its transpose made when the tensor is prepared;
+ * BF16x3 rank <= 64: three single-layout passes). d_grads[n]: shape[n] x rank.
  * loss may be NULL: no synchronization, and a device wait that ran out
  * (TSR_E_TIMEOUT) is reported by the context's next synchronizing call;
  * otherwise the call synchronizes and reports it. */

@@ -38,9 +38,10 @@ struct tsr_dense {
   bool d3_three = false;  // the view suits the single-layout 3-way MTTKRP
   bool d3_two = false;    // the view suits the two-sided contraction
   tsr::Dense3 d3{};
-  // FP32 tensors of 3 or more modes: the same view as a 2-way tensor
-  // (A, C = I_{N-2} I_{N-1}); its mode-0 operand is X (or a padded copy), its
-  // mode-1 operand the transposed copy (owned[2N + 2], owned[2N + 3])
+  // FP32 tensors of 3 or more modes: T and P as mode-0 MTTKRPs. vops[0] is X
+  // as the 3-way tensor (A, I_{N-2}, I_{N-1}) (X itself, or a padded copy);
+  // vops[1] is X's transpose (C x A, C = I_{N-2} I_{N-1}) as the tensor
+  // (C, I_0, .., I_{N-3}). Buffers in owned[2N + 2], owned[2N + 3].
   bool v2_on = false;
   int64_t v2_shape[2] = {0, 0};
   tsr::ModeOperand vops[2];
@@ -820,6 +821,7 @@ int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, cons
       vshape[1] * vshape[2] < INT32_MAX) {
     const int64_t v2[2] = {vshape[0], vshape[1] * vshape[2]};
     for (int m = 0; m < 2; ++m) {
+      // operand m: the 2-way view's mode-m unfolding (X, or its transpose)
       size_t ab, bb;
       mode_operand_bytes(make_unfolding(2, v2, m), precision, &ab, &bb);
       void* buf = nullptr;
@@ -831,6 +833,15 @@ int tsr_dense_create_dev_f32(tsr_ctx* ctx, const float* d_tensor, int ndim, cons
       int rc = prepare_mode_into(ctx, d_tensor, 2, v2, m, precision, buf, nullptr, &d->vops[m]);
       if (rc != TSR_OK) return cleanup(rc);
     }
+    // the same bytes read as mode-0 unfoldings of finer tensors (their row
+    // strides equal the 2-way view's: round_up(cols, 8)), so that the FP32
+    // kernel forms the Khatri-Rao rows from the factors and may take its
+    // run-scaled form over the fastest other mode
+    d->vops[0].u = make_unfolding(3, vshape, 0);
+    int64_t tshape[kMaxModes];
+    tshape[0] = v2[1];
+    for (int p = 0; p < ndim - 2; ++p) tshape[1 + p] = shape[p];
+    d->vops[1].u = make_unfolding(ndim - 1, tshape, 0);
     d->v2_on = true;
     d->v2_shape[0] = v2[0];
     d->v2_shape[1] = v2[1];
@@ -1024,38 +1035,32 @@ int tsr_cp_loss_grad_dev_f32(tsr_ctx* ctx, const tsr_dense* X, const float* cons
     return contract_grad(ts.T, ts.P);
   }
   if (X->v2_on && R <= 32) {
-    // FP32: X as the 2-way tensor (A, C). T is that view's mode-0 MTTKRP with
-    // W = KR(U_{N-2}, U_{N-1}), P its mode-1 MTTKRP with V = KR(U_0 ..
-    // U_{N-3}): two passes over X (the second over its transposed copy)
+    // FP32: T is the mode-0 MTTKRP of X as (A, I_{N-2}, I_{N-1}), P that of
+    // X's transpose as (C, I_0, .., I_{N-3}): two passes over X's bytes
     // instead of one per mode, and half the FLOPs of N MTTKRPs
     const int64_t A = X->v2_shape[0], C = X->v2_shape[1];
-    void *vp, *vq, *wp, *tp;
-    TSR_TRY(slot_get(ctx, SLOT_MISC1, sizeof(float) * A * R, &vp));
-    TSR_TRY(slot_get(ctx, SLOT_MISC3, sizeof(float) * A * R, &vq));
-    TSR_TRY(slot_get(ctx, SLOT_MISC2, sizeof(float) * C * R, &wp));
+    void* tp;
     TSR_TRY(slot_get(ctx, SLOT_MISC0, sizeof(float) * (A + C) * R, &tp));
-    const float* V = d_factors[0];
-    int64_t vrows = X->shape[0];
-    float* bufs[2] = {(float*)vp, (float*)vq};
-    for (int p = 1; p < N - 2; ++p) {
-      float* dst = bufs[p & 1];
-      TSR_TRY(launch_khatri_rao(ctx, V, vrows, d_factors[p], X->shape[p], R, dst));
-      V = dst;
-      vrows *= X->shape[p];
+    FactorTable f0{}, f1{};
+    f0.ptr[0] = d_factors[0];  // the output mode's slot (not read)
+    f0.rows[0] = A;
+    f0.ptr[1] = d_factors[N - 2];
+    f0.rows[1] = X->shape[N - 2];
+    f0.ptr[2] = d_factors[N - 1];
+    f0.rows[2] = X->shape[N - 1];
+    f1.ptr[0] = d_factors[0];  // not read
+    f1.rows[0] = C;
+    for (int p = 0; p < N - 2; ++p) {
+      f1.ptr[1 + p] = d_factors[p];
+      f1.rows[1 + p] = X->shape[p];
     }
-    TSR_TRY(launch_khatri_rao(ctx, d_factors[N - 2], X->shape[N - 2], d_factors[N - 1],
-                              X->shape[N - 1], R, (float*)wp));
-    FactorTable vt{};
-    vt.ptr[0] = V;
-    vt.rows[0] = A;
-    vt.ptr[1] = (const float*)wp;
-    vt.rows[1] = C;
     float* T = (float*)tp;
     float* P = T + A * R;
     for (int v = 0; v < 2; ++v) {
       float* partials;
       int splits;
-      TSR_TRY(run_mttkrp_partials(ctx, X->vops[v], vt, R, TSR_PREC_FP32, &partials, &splits));
+      TSR_TRY(run_mttkrp_partials(ctx, X->vops[v], v == 0 ? f0 : f1, R, TSR_PREC_FP32,
+                                  &partials, &splits));
       TSR_TRY(launch_mttkrp_reduce(ctx, partials, splits, (v == 0 ? A : C) * R, v == 0 ? T : P));
     }
     return contract_grad(T, P);
