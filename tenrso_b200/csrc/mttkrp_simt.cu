@@ -7,6 +7,8 @@
 // Replaces the i/r/j triple loop of crates/tenrso-kernels/src/mttkrp.rs:135-143
 // (same sum, different association: per-split partial sums, then a sum over
 // splits).
+#include <algorithm>
+
 #include "kr.cuh"
 #include "mttkrp.cuh"
 
@@ -421,8 +423,13 @@ SplitPlan plan_simt(const tsr_ctx* ctx, int64_t rows, int64_t K, int R, int64_t 
     // full wave at two CTAs per SM
     const int64_t mt = ceil_div(rows, RUN_BM), nt = ceil_div(R, p.bn);
     const int64_t steps = (K / L) * (round_up(L, 32) / 32);
+    // rounded up (a grid short of the unreserved slots leaves SMs idle), but
+    // within the physical slots so that the grid stays one wave
+    const int64_t tiles = mt * nt;
     const int64_t want = std::max<int64_t>(
-        1, std::min<int64_t>(steps, (int64_t)(ctx->sm_count - ctx->reserve_sms) * 2 / (mt * nt)));
+        1, std::min<int64_t>({steps,
+                              ceil_div((int64_t)(ctx->sm_count - ctx->reserve_sms) * 2, tiles),
+                              (int64_t)ctx->sm_count * 2 / tiles}));
     const int64_t per = ceil_div(steps, want);
     p.run_length = (int)L;
     p.k_per_split = per;
